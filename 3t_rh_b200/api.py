@@ -1,0 +1,452 @@
+"""Host-side mirror of the reference's Rust API for the 3T_RH hot path.
+
+Names, argument meaning and error behaviour follow colinhu123/3T_RH:
+  GridInfo, Field, Polygon, CircularArc/ArcOverride, BCType   (field1.rs, geometry.rs, bc1.rs)
+  GhostGrid.build                                              (ghost.rs:50-118)
+  l, rk3_ssp, calc_global_dt                                   (main.rs:135, 351, 375)
+Every computation runs in librh3t (include/rh3t.h): the geometry / ghost-grid
+build on the host in C++, the operator and the time stepping on the GPU.
+Where the reference panics, these functions raise RH3TError carrying the
+reference's message.
+"""
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import _lib
+
+FLUID_INSIDE, FLUID_OUTSIDE = 0, 1
+OUTER, INNER = 0, 1
+
+
+class RH3TError(RuntimeError):
+    """A failure the reference reports with panic! (main.rs:30-33, ghost.rs:229-263, bc1.rs:467-469, ...)."""
+
+    def __init__(self, code, message, stage=0, step=0, i=0, j=0, ghost=-1):
+        self.code, self.stage, self.step, self.i, self.j, self.ghost = code, stage, step, i, j, ghost
+        self.kind = _lib.STATUS_NAMES.get(code, str(code))
+        super().__init__(f"{message} [{self.kind}; step {step}, stage {stage}, idx ({i}, {j}), ghost {ghost}]")
+
+
+def _arr(a, dtype):
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+def _ptr(a):
+    return a.ctypes.data if a is not None and a.size else None
+
+
+# ------------------------------------------------------------------ bc1.rs:17-28
+class BCType:
+    REFLECTIVE_WALL, WALL, PERIODIC, CONSTANT, TIME_DEPENDENT, OUTFLOW, ZEROTH_ORDER, FAR_FIELD = range(8)
+
+    def __init__(self, kind, state=None, p_inf=0.0, sigma=0.0, l_domain=1.0, td_x0=0.0, td_speed=0.0,
+                 td_left=None, td_right=None):
+        self.kind = kind
+        self.state = np.zeros(6) if state is None else np.asarray(state, dtype=np.float64)
+        self.p_inf, self.sigma, self.l_domain = float(p_inf), float(sigma), float(l_domain)
+        self.td_x0, self.td_speed = float(td_x0), float(td_speed)
+        self.td_left = np.zeros(6) if td_left is None else np.asarray(td_left, dtype=np.float64)
+        self.td_right = np.zeros(6) if td_right is None else np.asarray(td_right, dtype=np.float64)
+
+    @classmethod
+    def ReflectiveWall(cls):
+        return cls(cls.REFLECTIVE_WALL)
+
+    @classmethod
+    def Wall(cls):
+        return cls(cls.WALL)
+
+    @classmethod
+    def Periodic(cls):
+        return cls(cls.PERIODIC)
+
+    @classmethod
+    def Constant(cls, state):
+        return cls(cls.CONSTANT, state=state)
+
+    @classmethod
+    def TimeDependent(cls, x0, speed, left, right):
+        """The reference's closure type (bc1.rs:14) restricted to its one use
+        (init.rs:61-65): U = left if P0.x <= x0 + speed*t else right."""
+        return cls(cls.TIME_DEPENDENT, td_x0=x0, td_speed=speed, td_left=left, td_right=right)
+
+    @classmethod
+    def Outflow(cls, p_inf, sigma, l_domain):
+        return cls(cls.OUTFLOW, p_inf=p_inf, sigma=sigma, l_domain=l_domain)
+
+    @classmethod
+    def ZerothOrder(cls):
+        return cls(cls.ZEROTH_ORDER)
+
+    @classmethod
+    def FarField(cls, state):
+        return cls(cls.FAR_FIELD, state=state)
+
+    def to_c(self):
+        b = _lib.BC()
+        b.kind = self.kind
+        for k in range(6):
+            b.state[k] = self.state[k]
+            b.td_left[k] = self.td_left[k]
+            b.td_right[k] = self.td_right[k]
+        b.p_inf, b.sigma, b.l_domain, b.td_x0, b.td_speed = self.p_inf, self.sigma, self.l_domain, self.td_x0, \
+            self.td_speed
+        return b
+
+
+# ------------------------------------------------------------------ constant.rs
+class Params:
+    """constant.rs values as runtime parameters (defaults = the reference's)."""
+    FIELDS = _lib.PARAM_FIELDS
+
+    def __init__(self, **kw):
+        self.gamma_e = self.gamma_i = self.gamma_r = 1.4
+        self.cve = self.cvi = self.a_rad = 1.0
+        self.kappa_e = self.kappa_i = self.kappa_r = 0.0
+        self.omega_ei = self.omega_er = 0.0
+        self.lambda_, self.weno_q, self.eps, self.periodic_ly = 0.5, 10.0, 1e-12, 0.5
+        for k, v in kw.items():
+            if k not in self.FIELDS:
+                raise TypeError(f"unknown parameter {k}")
+            setattr(self, k, float(v))
+
+    def to_c(self):
+        p = _lib.Params()
+        for k in self.FIELDS:
+            setattr(p, k, getattr(self, k))
+        return p
+
+    def as_array(self):
+        return np.array([getattr(self, k) for k in self.FIELDS])
+
+
+# ------------------------------------------------------------------ field1.rs:6-73
+class GridInfo:
+    def __init__(self, nx, ny, dx, dy, x0, y0):
+        assert nx > 0 and ny > 0 and dx > 0.0 and dy > 0.0
+        self.nx, self.ny, self.dx, self.dy, self.x0, self.y0 = int(nx), int(ny), float(dx), float(dy), float(x0), \
+            float(y0)
+
+    def x(self, i):
+        return self.x0 + float(i) * self.dx
+
+    def y(self, j):
+        return self.y0 + float(j) * self.dy
+
+    def len(self):
+        return self.nx * self.ny
+
+    def is_in_domain(self, idx):
+        i, j = idx
+        return 0 <= i < self.nx and 0 <= j < self.ny
+
+    def coord2idx(self, p):
+        return (int(_round_half_away((p[0] - self.x0) / self.dx)), int(_round_half_away((p[1] - self.y0) / self.dy)))
+
+    def to_c(self):
+        return _lib.Grid(self.nx, self.ny, self.dx, self.dy, self.x0, self.y0)
+
+
+def _round_half_away(v):
+    return math.floor(v + 0.5) if v >= 0 else -math.floor(-v + 0.5)
+
+
+# ------------------------------------------------------------------ geometry.rs
+class Polygon:
+    def __init__(self, points, fluid=FLUID_INSIDE):
+        self.points = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 2)
+        self.fluid = fluid
+
+
+class CircularArc:
+    """geometry.rs:492-549: kept as its three construction points; the arc
+    itself (centre, radius, angles) is formed in librh3t."""
+
+    def __init__(self, start, mid, end, fluid):
+        self.start, self.mid, self.end, self.fluid = tuple(start), tuple(mid), tuple(end), fluid
+
+    @classmethod
+    def from_three_points(cls, start, mid, end, fluid):
+        return cls(start, mid, end, fluid)
+
+
+class ArcOverride:
+    def __init__(self, side_start, side_end, arc, boundary=OUTER):
+        self.side_start, self.side_end, self.arc, self.boundary = int(side_start), int(side_end), arc, boundary
+
+    def contains_side(self, side):
+        return self.side_start <= side <= self.side_end
+
+    def to_c(self):
+        a = _lib.Arc()
+        a.boundary, a.side_start, a.side_end, a.fluid_side = self.boundary, self.side_start, self.side_end, \
+            self.arc.fluid
+        for k in range(2):
+            a.start[k], a.mid[k], a.end[k] = self.arc.start[k], self.arc.mid[k], self.arc.end[k]
+        return a
+
+
+# ------------------------------------------------------------------ field1.rs:75-136
+class Field:
+    """Field: grid, node values (nx*ny x 6, linear index i*ny+j), the two
+    bounding polygons with one BCType per side, time, fluid mask, arcs."""
+
+    def __init__(self, grid, bc_inner, bc_outer, value, outer_bound, inner_bound, time=0.0, params=None):
+        assert outer_bound.fluid == FLUID_INSIDE, "Wrong outer boundary setting"
+        assert inner_bound.fluid == FLUID_OUTSIDE, "Wrong inner boundary setting"
+        assert len(bc_inner) == len(inner_bound.points)
+        assert len(bc_outer) == len(outer_bound.points)
+        self.grid = grid
+        self.params = params if params is not None else Params()
+        self.outer_bound, self.inner_bound = outer_bound, inner_bound
+        self.bc_inner, self.bc_outer = list(bc_inner), list(bc_outer)
+        self.time = float(time)
+        self.outer_arcs, self.inner_arcs = [], []
+        v = np.asarray(value, dtype=np.float64)
+        self.value = np.tile(v.reshape(1, 6), (grid.len(), 1)) if v.size == 6 else _arr(v.reshape(-1, 6), np.float64)
+        with _Geom(self, arcs=False) as g:
+            self.fluid = g.fluid_mask()
+
+    def is_in_domain(self, idx):
+        i, j = idx
+        return self.grid.is_in_domain(idx) and bool(self.fluid[i * self.grid.ny + j])
+
+    def linear_index(self, idx):
+        return idx[0] * self.grid.ny + idx[1]
+
+    def set(self, idx, value):
+        assert self.is_in_domain(idx), f"cannot write ghost cell {idx}"
+        self.value[self.linear_index(idx)] = value
+
+    def get_inside(self, idx):
+        return self.value[self.linear_index(idx)]
+
+    def empty_like(self):
+        f = object.__new__(Field)
+        f.__dict__.update(self.__dict__)
+        f.value = np.zeros_like(self.value)
+        return f
+
+
+class _Geom:
+    """Owner of an rh3t_geom handle (the C++ host build)."""
+
+    def __init__(self, field, arcs=True):
+        L = _lib.load()
+        self.L = L
+        ob, ib = field.outer_bound, field.inner_bound
+        self._keep = []
+        obc = (_lib.BC * len(field.bc_outer))(*[b.to_c() for b in field.bc_outer])
+        ibc = (_lib.BC * max(1, len(field.bc_inner)))(*[b.to_c() for b in field.bc_inner])
+        arc_list = (field.outer_arcs + field.inner_arcs) if arcs else []
+        carcs = (_lib.Arc * max(1, len(arc_list)))(*[a.to_c() for a in arc_list])
+        oxy, ixy = _arr(ob.points, np.float64), _arr(ib.points, np.float64)
+        self._keep += [obc, ibc, carcs, oxy, ixy]
+        h = C.c_void_p()
+        grid, prm = field.grid.to_c(), field.params.to_c()
+        rc = L.rh3t_geom_create(C.byref(grid), C.byref(prm), len(ob.points), oxy.ctypes.data, ob.fluid,
+                                C.addressof(obc), len(ib.points), ixy.ctypes.data, ib.fluid, C.addressof(ibc),
+                                len(arc_list), C.addressof(carcs), C.byref(h))
+        if rc:
+            raise RH3TError(rc, "geometry set-up failed")
+        self.h = h
+        self.n = field.grid.len()
+
+    def fluid_mask(self):
+        out = np.zeros(self.n, dtype=np.uint8)
+        self.L.rh3t_geom_fluid_mask(self.h, out.ctypes.data)
+        return out.astype(bool)
+
+    def close(self):
+        if self.h:
+            self.L.rh3t_geom_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+# ------------------------------------------------------------------ ghost.rs:30-118
+class GhostGrid:
+    """Static ghost layout: per ghost its grid index, final projection
+    (P0, outward normal, signed distance), boundary and selected side, and for
+    Wall / Outflow / FarField ghosts the GhostBC tables (bc1.rs:50-57)."""
+
+    @classmethod
+    def build(cls, field, n_threads=0, with_access=False):
+        g = cls()
+        with _Geom(field) as geom:
+            rc = geom.L.rh3t_geom_build_ghosts(geom.h, n_threads)
+            if rc:
+                raise RH3TError(rc, geom.L.rh3t_geom_last_error(geom.h).decode())
+            v = _lib.GhostTable()
+            geom.L.rh3t_geom_ghost_table(geom.h, C.byref(v))
+            n, m = v.n_ghosts, v.n_heavy
+
+            def cp(ptr, count, dtype):
+                if count == 0:
+                    return np.zeros(0, dtype=dtype)
+                buf = (C.c_char * (count * np.dtype(dtype).itemsize)).from_address(ptr)
+                return np.frombuffer(buf, dtype=dtype).copy()
+
+            g.idx = cp(v.idx, 2 * n, np.int32).reshape(n, 2)
+            g.boundary = cp(v.boundary, n, np.int32)
+            g.side = cp(v.side, n, np.int32)
+            g.proj = cp(v.proj, 5 * n, np.float64).reshape(n, 5)
+            g.pre = cp(v.pre, n, np.int32)
+            g.nearest = cp(v.nearest, 2 * m, np.int32).reshape(m, 2)
+            g.stencil = cp(v.stencil, 55 * m, np.uint32).reshape(m, 55)
+            g.s = cp(v.s, 979 * m, np.float64).reshape(m, 979)
+            g.w = cp(v.w, 225 * m, np.float64).reshape(m, 225)
+            g.d = cp(v.d, 5 * m, np.float64).reshape(m, 5)
+            if with_access:
+                g.access = np.zeros(field.grid.len() * 17, np.uint32)
+                geom.L.rh3t_geom_access_table(geom.h, g.access.ctypes.data)
+                g.access = g.access.reshape(-1, 17)
+        return g
+
+    @classmethod
+    def from_arrays(cls, idx, boundary, side, proj, pre, nearest, stencil, s, w, d):
+        """A GhostGrid handed over from another builder (the reference's Rust
+        GhostGrid, or any table in the same layout)."""
+        g = cls()
+        g.idx = _arr(idx, np.int32).reshape(-1, 2)
+        g.boundary, g.side, g.pre = _arr(boundary, np.int32), _arr(side, np.int32), _arr(pre, np.int32)
+        g.proj = _arr(proj, np.float64).reshape(-1, 5)
+        g.nearest = _arr(nearest, np.int32).reshape(-1, 2)
+        g.stencil = _arr(stencil, np.uint32).reshape(-1, 55)
+        g.s, g.w, g.d = (_arr(s, np.float64).reshape(-1, 979), _arr(w, np.float64).reshape(-1, 225),
+                         _arr(d, np.float64).reshape(-1, 5))
+        return g
+
+    def len(self):
+        return len(self.boundary)
+
+    def n_heavy(self):
+        return len(self.nearest)
+
+    def to_c(self):
+        t = _lib.GhostTable()
+        t.n_ghosts, t.n_heavy = self.len(), self.n_heavy()
+        t.idx, t.boundary, t.side, t.proj, t.pre = (_ptr(self.idx), _ptr(self.boundary), _ptr(self.side),
+                                                    _ptr(self.proj), _ptr(self.pre))
+        t.nearest, t.stencil, t.s, t.w, t.d = (_ptr(self.nearest), _ptr(self.stencil), _ptr(self.s), _ptr(self.w),
+                                               _ptr(self.d))
+        return t
+
+
+# ------------------------------------------------------------------ device solver
+class Solver:
+    """Device copy of a Field + GhostGrid + the l() scratch (main.rs:45-67):
+    one rh3t_ctx on one CUDA stream."""
+
+    def __init__(self, field, ghosts, device=0, exact=False):
+        self.L = _lib.load(exact)
+        self.exact = exact
+        self.grid = field.grid
+        self.n_ghosts = ghosts.len()
+        obc = (_lib.BC * len(field.bc_outer))(*[b.to_c() for b in field.bc_outer])
+        ibc = (_lib.BC * max(1, len(field.bc_inner)))(*[b.to_c() for b in field.bc_inner])
+        fluid = _arr(field.fluid, np.uint8)
+        table = ghosts.to_c()
+        h = C.c_void_p()
+        grid, prm = field.grid.to_c(), field.params.to_c()
+        rc = self.L.rh3t_create(C.byref(grid), C.byref(prm), fluid.ctypes.data, len(field.bc_outer),
+                                C.addressof(obc), len(field.bc_inner), C.addressof(ibc), C.byref(table), device,
+                                C.byref(h))
+        if rc:
+            raise RH3TError(rc, "rh3t_create failed")
+        self.h = h
+        self.upload(field)
+
+    def _check(self, rc):
+        if rc:
+            e = _lib.Error()
+            self.L.rh3t_last_error(self.h, C.byref(e))
+            raise RH3TError(e.code or rc, e.message.decode(), e.stage, e.step, e.i, e.j, e.ghost)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.rh3t_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def upload(self, field):
+        v = _arr(field.value, np.float64)
+        self._check(self.L.rh3t_upload_state(self.h, v.ctypes.data, field.time))
+
+    def download(self, field=None):
+        out = np.zeros((self.grid.len(), 6))
+        t = C.c_double()
+        self._check(self.L.rh3t_download_state(self.h, out.ctypes.data, C.byref(t)))
+        if field is not None:
+            fl = field.fluid
+            field.value[fl] = out[fl]
+            field.time = t.value
+        return out, t.value
+
+    def l(self, with_ghosts=False):
+        rhs = np.zeros((self.grid.len(), 6))
+        gv = np.zeros((self.n_ghosts, 6)) if with_ghosts else None
+        self._check(self.L.rh3t_l(self.h, rhs.ctypes.data, _ptr(gv)))
+        return (rhs, gv) if with_ghosts else rhs
+
+    def calc_global_dt(self):
+        d = C.c_double()
+        self._check(self.L.rh3t_calc_global_dt(self.h, C.byref(d)))
+        return d.value
+
+    def rk3_ssp(self, dt):
+        self._check(self.L.rh3t_rk3_ssp(self.h, float(dt)))
+
+    def advance(self, nsteps, cfl_factor=0.05, t_final=math.inf, graph=True):
+        self._check(self.L.rh3t_advance(self.h, int(nsteps), float(cfl_factor), float(t_final), int(bool(graph))))
+
+    def step_host(self, value, time, cfl_factor=0.05):
+        """One reference time-loop iteration on a host value array (in place)."""
+        t = C.c_double(time)
+        dt = C.c_double()
+        self._check(self.L.rh3t_step_host(self.h, value.ctypes.data, C.byref(t), float(cfl_factor), C.byref(dt)))
+        return t.value, dt.value
+
+    def last_dt(self):
+        d = C.c_double()
+        self._check(self.L.rh3t_last_dt(self.h, C.byref(d)))
+        return d.value
+
+    def synchronize(self):
+        self._check(self.L.rh3t_synchronize(self.h))
+
+    @property
+    def kernel_launches(self):
+        return int(self.L.rh3t_kernel_launches(self.h))
+
+    @property
+    def stream(self):
+        return self.L.rh3t_stream(self.h)
+
+
+# ------------------------------------------------------------------ main.rs functions
+def l(u, ghosts, solver):
+    """main.rs:135-305: semi-discrete operator of u; returns rhs (nx*ny x 6)."""
+    solver.upload(u)
+    return solver.l()
+
+
+def calc_global_dt(u, solver):
+    """main.rs:375-408"""
+    solver.upload(u)
+    return solver.calc_global_dt()
+
+
+def rk3_ssp(u, ghosts, dt, solver):
+    """main.rs:351-373: advances the host Field u in place by one SSP-RK3 step."""
+    solver.upload(u)
+    solver.rk3_ssp(dt)
+    solver.download(u)

@@ -1,0 +1,151 @@
+"""Initial conditions / domains of the workloads (the builders the reference
+keeps in init.rs, restated for inputs of the solver).
+
+  init_cylinder     init.rs:116-510 with mesh width, Mach number and arc shift
+                    as parameters (reference: h = 1/40, M = 3, shift 0.0125)
+  init_double_mach  init.rs:26-113 (reference mesh width 1/320)
+  planar_shock      translating Mach-2 shock, y-periodic (no reference builder)
+  rect_field        bc1.rs:1641-1702 test fixture (one BC kind on all sides)
+"""
+import math
+
+import numpy as np
+
+from .api import (FLUID_INSIDE, FLUID_OUTSIDE, ArcOverride, BCType, CircularArc, Field, GridInfo, Params,
+                  Polygon)
+
+
+def euler_to_three_energy(rho, ux, uy, p, gamma):
+    """init.rs:7-24: equal split of the total energy."""
+    kinetic = 0.5 * rho * (ux * ux + uy * uy)
+    e_total = p / (gamma - 1.0) + kinetic
+    return np.array([rho, rho * ux, rho * uy, e_total / 3.0, e_total / 3.0, e_total / 3.0])
+
+
+def _dummy_inner():
+    return Polygon([(-1002.0, -1002.0), (-1001.0, -1002.0), (-1001.0, -1001.0), (-1002.0, -1001.0)], FLUID_OUTSIDE)
+
+
+def freestream(mach=3.0):
+    gamma, rho_inf, p_inf = 1.4, 1.0, 1.0
+    a_inf = math.sqrt(gamma * p_inf / rho_inf)
+    return euler_to_three_energy(rho_inf, mach * a_inf, 0.0, p_inf, gamma)
+
+
+def init_cylinder(h=1.0 / 40.0, mach=3.0, shift=0.0125, params=None):
+    u_inf = freestream(mach)
+    x0, y0, lx, ly = -3.0, -6.0, 3.0, 12.0
+    nx = int(_round(lx / h)) + 1
+    ny = int(_round(ly / h)) + 1
+    grid = GridInfo(nx, ny, h, h, x0, y0)
+    pts = [(-3.0, -6.0), (0.0, -6.0)]
+    bcs = [BCType.FarField(u_inf)]
+    pts.append((0.0, -1.0 + shift))
+    bcs.append(BCType.FarField(u_inf))
+    n_arc = 360
+    arc_start = len(bcs)
+    for k in range(1, n_arc + 1):
+        s = float(k) / float(n_arc)
+        theta = -0.5 * math.pi - math.pi * s
+        pts.append((math.cos(theta), math.sin(theta) + shift))
+        bcs.append(BCType.ReflectiveWall())
+    arc_end = len(bcs) - 1
+    arc = CircularArc.from_three_points((0.0, -1.0 + shift), (-1.0, 0.0 + shift), (0.0, 1.0 + shift), FLUID_OUTSIDE)
+    pts.append((0.0, 6.0))
+    bcs.append(BCType.FarField(u_inf))
+    pts.append((-3.0, 6.0))
+    bcs.append(BCType.FarField(u_inf))
+    bcs.append(BCType.FarField(u_inf))
+    f = Field(grid, [BCType.Wall()] * 4, bcs, np.zeros(6), Polygon(pts, FLUID_INSIDE), _dummy_inner(), 0.0,
+              params=params)
+    f.outer_arcs.append(ArcOverride(arc_start, arc_end, arc))
+    f.value[f.fluid] = u_inf
+    return f
+
+
+def init_double_mach(h=1.0 / 320.0, params=None):
+    sqrt3 = math.sqrt(3.0)
+    a = (-0.5 - sqrt3 / 12.0, 0.0)
+    b = (0.0, 0.0)
+    c = (23.0 * sqrt3 / 12.0, 23.0 / 12.0)
+    d = (c[0], 23.0 / 12.0 + sqrt3 / 2.0)
+    e = (a[0], d[1])
+    x0, y0, lx, ly = a[0], 0.0, c[0] - a[0], d[1]
+    nx = int(math.ceil(lx / h)) + 1
+    ny = int(math.ceil(ly / h)) + 1
+    grid = GridInfo(nx, ny, h, h, x0, y0)
+    pre = euler_to_three_energy(1.4, 0.0, 0.0, 1.0, 1.4)
+    post = euler_to_three_energy(8.0, 8.25, 0.0, 116.5, 1.4)
+    bcs = [BCType.Constant(post), BCType.Wall(), BCType.Constant(pre), BCType.ZerothOrder(), BCType.Constant(post)]
+    f = Field(grid, [BCType.Wall()] * 4, bcs, np.zeros(6), Polygon([a, b, c, d, e], FLUID_INSIDE), _dummy_inner(),
+              0.0, params=params)
+    for i in range(nx):
+        row = np.arange(ny) + i * ny
+        fl = f.fluid[row]
+        f.value[row[fl]] = post if grid.x(i) <= 0.0 else pre
+    return f
+
+
+def _solve_temperature(target, ce, ci, cr, rho, P):
+    def fn(T):
+        te, ti, tr = ce * T, ci * T, cr * T
+        return P.cve * te + P.cvi * ti + P.a_rad * ((tr * tr) * (tr * tr)) / rho - target
+
+    lo, hi = 0.0, 1.0
+    while fn(hi) < 0.0:
+        hi *= 2.0
+    for _ in range(200):
+        mid = 0.5 * (lo + hi)
+        if fn(mid) < 0.0:
+            lo = mid
+        else:
+            hi = mid
+        if hi - lo <= 0.0:
+            break
+    return 0.5 * (lo + hi)
+
+
+def _three_temp_state(rho, u, v, te, ti, tr, P):
+    e_e, e_i, e_r = P.cve * te, P.cvi * ti, P.a_rad * ((tr * tr) * (tr * tr)) / rho
+    k = rho * (u * u + v * v) / 6.0
+    return np.array([rho, rho * u, rho * v, rho * e_e + k, rho * e_i + k, rho * e_r + k])
+
+
+def planar_shock(nx=1024, ny=8, lx=4.0, ly=0.03125, x_shock=1.0, mach=2.0, sigma=0.25, params=None):
+    """Mach-`mach` shock at x_shock moving into (rho, u, p) = (1, 0, 1),
+    gamma = 1.4 Rankine-Hugoniot on the total energy; pre-shock
+    Te = Ti = Tr, post-shock Te:Ti:Tr = 1 : 1.5 : 0.8. Bottom/top Periodic,
+    right Outflow(p_inf = 1, sigma, l_domain = lx), left FarField(post)."""
+    P = params if params is not None else Params(periodic_ly=ly)
+    grid = GridInfo(nx, ny, lx / float(nx), ly / float(ny), 0.0, 0.0)
+    g, rho1, u1, p1 = 1.4, 1.0, 0.0, 1.0
+    c1 = math.sqrt(g * p1 / rho1)
+    m2 = mach * mach
+    rho2 = rho1 * (g + 1.0) * m2 / ((g - 1.0) * m2 + 2.0)
+    p2 = p1 * (2.0 * g * m2 - (g - 1.0)) / (g + 1.0)
+    ws = mach * c1
+    u2 = ws * (1.0 - rho1 / rho2)
+    t1 = _solve_temperature(p1 / ((g - 1.0) * rho1), 1.0, 1.0, 1.0, rho1, P)
+    t2 = _solve_temperature(p2 / ((g - 1.0) * rho2), 1.0, 1.5, 0.8, rho2, P)
+    pre = _three_temp_state(rho1, u1, 0.0, t1, t1, t1, P)
+    post = _three_temp_state(rho2, u2, 0.0, t2, 1.5 * t2, 0.8 * t2, P)
+    bcs = [BCType.Periodic(), BCType.Outflow(p1, sigma, lx), BCType.Periodic(), BCType.FarField(post)]
+    f = Field(grid, [BCType.Wall()] * 4, bcs, np.zeros(6), Polygon([(0.0, 0.0), (lx, 0.0), (lx, ly), (0.0, ly)],
+                                                                  FLUID_INSIDE), _dummy_inner(), 0.0, params=P)
+    for i in range(nx):
+        row = np.arange(ny) + i * ny
+        fl = f.fluid[row]
+        f.value[row[fl]] = post if grid.x(i) < x_shock else pre
+    return f
+
+
+def rect_field(nx, ny, lx, ly, value, kind=BCType.WALL, params=None):
+    grid = GridInfo(nx, ny, lx / float(nx), ly / float(ny), 0.0, 0.0)
+    b = BCType(kind, state=value)
+    return Field(grid, [BCType.Wall()] * 4, [b] * 4, value,
+                 Polygon([(0.0, 0.0), (lx, 0.0), (lx, ly), (0.0, ly)], FLUID_INSIDE), _dummy_inner(), 0.0,
+                 params=params)
+
+
+def _round(v):
+    return math.floor(v + 0.5) if v >= 0 else -math.floor(-v + 0.5)

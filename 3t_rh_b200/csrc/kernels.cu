@@ -1,0 +1,681 @@
+// rh3t device kernels (sm_100a, FP64). One launch of each kernel covers all
+// instances of a context or batch: cell and face kernels walk a list of
+// 128-wide tiles, the ghost kernel a list of ghost records, so the plain
+// solver is simply a batch of one.
+//
+// Per RK stage: k_ghosts (ghost.rs:199-268) -> k_flux (main.rs:165-246) ->
+// k_rhs_stage (main.rs:251-349). Per step: k_dt (main.rs:375-408, dt.rs)
+// first. dt, stage times and RK coefficients never leave the device.
+#include "kernels.cuh"
+#include "physics.cuh"
+
+namespace rh3t {
+
+__device__ __forceinline__ long long node_of(const Inst& I, int i, int j) {
+    return (long long)(i + RH3T_PAD) * I.nyp + (j + RH3T_PAD);
+}
+
+__device__ __forceinline__ void load6(const double* __restrict__ buf, long long plane, long long n, double s[6]) {
+#pragma unroll
+    for (int c = 0; c < 6; ++c) s[c] = buf[c * plane + n];
+}
+
+__device__ __forceinline__ bool has_error(const Inst& I) { return I.err->key != ~0ull; }
+
+__device__ __forceinline__ void report(const Inst& I, int phase, int code, unsigned int index) {
+    unsigned long long step = (unsigned long long)I.sc->step;
+    unsigned long long key = (step << 40) | ((unsigned long long)phase << 37) | ((unsigned long long)code << 32) |
+                             (unsigned long long)index;
+    atomicMin(&I.err->key, key);
+}
+
+__device__ __forceinline__ const double* stage_src(const Inst& I, int stage) {
+    return stage == 0 ? I.U : (stage == 1 ? I.A : I.B);
+}
+
+// ------------------------------------------------------------------ ghosts
+// 6 threads per ghost (threadIdx.x = characteristic component c), 32 ghosts
+// per block. Heavy ghosts (Wall / Outflow / FarField): thread c forms the c-th
+// characteristic data of the five E_r stencils, its smoothness indicators
+// beta_r = d^T S_r d and the V^(k) = w_{r,k} . d with the reference's
+// summation order (bc1.rs:193-255), once for all k (the reference repeats
+// this identical work for k = 0..4, bc1.rs:673-675). Thread 0 then applies
+// the BC rows, the Taylor expansion and the rotation (bc1.rs:690-924).
+struct GhostShared {
+    double L[6][6];
+    double R[6][6]; // R[col][row]
+    double lam[6];
+    double v[5][6];
+};
+
+__device__ __forceinline__ void matvec_cols(const double Rc[6][6], const double x[6], double out[6]) {
+    // out[i] = sum_j R[i][j] x[j], R stored by column: Rc[j][i]
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        double acc = 0.0;
+#pragma unroll
+        for (int j = 0; j < 6; ++j) acc += Rc[j][i] * x[j];
+        out[i] = acc;
+    }
+}
+
+__device__ __forceinline__ void matvec_rows(const double L[6][6], const double x[6], double out[6]) {
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        double acc = 0.0;
+#pragma unroll
+        for (int j = 0; j < 6; ++j) acc += L[i][j] * x[j];
+        out[i] = acc;
+    }
+}
+
+// bc1.rs:467-469 solve6 with LAPACK getrf/getrs semantics
+__device__ bool solve6(double A[6][6], double b[6]) {
+    int piv[6];
+    for (int j = 0; j < 6; ++j) {
+        int p = j;
+        double mx = fabs(A[j][j]);
+        for (int i = j + 1; i < 6; ++i)
+            if (fabs(A[i][j]) > mx) { mx = fabs(A[i][j]); p = i; }
+        piv[j] = p;
+        if (A[p][j] == 0.0) return false;
+        if (p != j)
+            for (int k = 0; k < 6; ++k) { double t = A[j][k]; A[j][k] = A[p][k]; A[p][k] = t; }
+        double rcp = 1.0 / A[j][j];
+        for (int i = j + 1; i < 6; ++i) A[i][j] *= rcp;
+        for (int k = j + 1; k < 6; ++k)
+            for (int i = j + 1; i < 6; ++i) A[i][k] -= A[i][j] * A[j][k];
+    }
+    for (int j = 0; j < 6; ++j)
+        if (piv[j] != j) { double t = b[j]; b[j] = b[piv[j]]; b[piv[j]] = t; }
+    for (int k = 0; k < 6; ++k)
+        for (int i = k + 1; i < 6; ++i) b[i] -= b[k] * A[i][k];
+    for (int k = 5; k >= 0; --k) {
+        b[k] /= A[k][k];
+        for (int i = 0; i < k; ++i) b[i] -= b[k] * A[i][k];
+    }
+    return true;
+}
+
+template <int R_>
+__device__ __forceinline__ void extrap_order(const double* __restrict__ buf, long long plane,
+                                             const int32_t* __restrict__ st, const double* __restrict__ S,
+                                             const double* __restrict__ W, const double Lc[6], double nx, double ny,
+                                             double& beta, double vk[5]) {
+    constexpr int m = (R_ + 1) * (R_ + 1);
+    double data[m];
+#pragma unroll
+    for (int a = 0; a < m; ++a) {
+        long long n = st[a];
+        double rho = buf[n], mx = buf[plane + n], my = buf[2 * plane + n];
+        double ee = buf[3 * plane + n], ei = buf[4 * plane + n], er = buf[5 * plane + n];
+        double mn = mx * nx + my * ny;
+        double mt = -mx * ny + my * nx;
+        data[a] = Lc[0] * rho + Lc[1] * mn + Lc[2] * mt + Lc[3] * ee + Lc[4] * ei + Lc[5] * er;
+    }
+    double b = 0.0;
+#pragma unroll
+    for (int a = 0; a < m; ++a) {
+        double acc = 0.0;
+#pragma unroll
+        for (int q = 0; q < m; ++q) acc += S[a * m + q] * data[q];
+        b += data[a] * acc;
+    }
+    beta = b;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        double v = 0.0;
+        if (k <= R_) {
+#pragma unroll
+            for (int a = 0; a < m; ++a) v += W[k * m + a] * data[a];
+        }
+        vk[k] = v;
+    }
+}
+
+__global__ void __launch_bounds__(192) k_ghosts(const Inst* __restrict__ insts, const GhostRec* __restrict__ recs,
+                                                int n_recs, const int32_t* __restrict__ hv_st,
+                                                const double* __restrict__ hv_s, const double* __restrict__ hv_w,
+                                                const double* __restrict__ hv_d, int stage) {
+    __shared__ GhostShared sh[32];
+    const int c = threadIdx.x;
+    const int gl = threadIdx.y;
+    const int g = blockIdx.x * 32 + gl;
+    const bool active = g < n_recs;
+    GhostRec R;
+    const Inst* Ip = nullptr;
+    bool heavy = false;
+    const double* buf = nullptr;
+    long long plane = 0;
+    bool skip = true;
+    if (active) {
+        R = recs[g];
+        Ip = &insts[R.inst];
+        skip = has_error(*Ip);
+        buf = stage_src(*Ip, stage);
+        plane = Ip->plane;
+        heavy = R.heavy >= 0;
+    }
+    if (active && !skip && !heavy) {
+        const Inst& I = *Ip;
+        double val;
+        const DevBC& bc = I.bcs[R.bc];
+        if (R.kind == BC_CONSTANT) {
+            val = bc.state[c];
+        } else if (R.kind == BC_TIME_DEPENDENT) {
+            double xs = bc.td_x0 + bc.td_speed * I.sc->t_stage[stage];
+            val = R.p0x <= xs ? bc.td_left[c] : bc.td_right[c];
+        } else if (R.kind == BC_REFLECTIVE_WALL) {
+            double s[6];
+            load6(buf, plane, R.src, s);
+            double mom_n = s[1] * R.nx + s[2] * R.ny;
+            val = c == 1 ? s[1] - 2.0 * mom_n * R.nx : (c == 2 ? s[2] - 2.0 * mom_n * R.ny : s[c]);
+        } else { // ZerothOrder, Periodic: copy of the source node
+            val = buf[c * plane + R.src];
+        }
+        if (!isfinite(val)) report(I, 1 + 2 * stage, 2, (unsigned)R.gid);
+        const_cast<double*>(buf)[c * plane + R.node] = val;
+    }
+    if (active && !skip && heavy) {
+        const Inst& I = *Ip;
+        const DevParams& P = I.P;
+        double s[6];
+        load6(buf, plane, R.src, s);
+        // bc1.rs:294-312 build_local_plain: nearest state rotated to (n, t)
+        double mom_n = s[1] * R.nx + s[2] * R.ny;
+        double mom_t = -s[1] * R.ny + s[2] * R.nx;
+        double s1[6] = {s[0], mom_n, mom_t, s[3], s[4], s[5]};
+        Prim d1 = prim_from_state(s1, P);
+        Roe q = roe_average(s1[0], d1, s1[0], d1, P);
+        double Lc[6];
+        l_row<0>(c, q, P, Lc);
+        double Rc[6], lam;
+        r_col<0>(c, q, P, Rc, lam);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) { sh[gl].L[c][k] = Lc[k]; sh[gl].R[c][k] = Rc[k]; }
+        sh[gl].lam[c] = lam;
+        const long long h = R.heavy;
+        const int32_t* st = hv_st + h * 55;
+        const double* S = hv_s + h * 979;
+        const double* W = hv_w + h * 225;
+        double beta[5], vk[5][5];
+        extrap_order<0>(buf, plane, st + 0, S + 0, W + 0, Lc, R.nx, R.ny, beta[0], vk[0]);
+        extrap_order<1>(buf, plane, st + 1, S + 1, W + 1, Lc, R.nx, R.ny, beta[1], vk[1]);
+        extrap_order<2>(buf, plane, st + 5, S + 17, W + 9, Lc, R.nx, R.ny, beta[2], vk[2]);
+        extrap_order<3>(buf, plane, st + 14, S + 98, W + 36, Lc, R.nx, R.ny, beta[3], vk[3]);
+        extrap_order<4>(buf, plane, st + 30, S + 354, W + 100, Lc, R.nx, R.ny, beta[4], vk[4]);
+        double alpha[5], asum = 0.0;
+#pragma unroll
+        for (int r = 0; r < 5; ++r) {
+            alpha[r] = hv_d[h * 5 + r] / pow(P.eps + beta[r], P.weno_q);
+            asum += alpha[r];
+        }
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+            double res = 0.0;
+#pragma unroll
+            for (int r = 0; r < 5; ++r) res += (alpha[r] / asum) * vk[r][k];
+            sh[gl].v[k][c] = res;
+        }
+    }
+    __syncthreads();
+    if (!(active && !skip && heavy) || c != 0) return;
+    const Inst& I = *Ip;
+    const DevParams& P = I.P;
+    GhostShared& G = sh[gl];
+    double u[5][6];
+    if (R.kind == BC_WALL) {
+        // bc1.rs:691-756
+        double A0[6][6], rhs0[6];
+        for (int i = 0; i < 6; ++i)
+            for (int k = 0; k < 6; ++k) A0[i][k] = G.L[i][k];
+        for (int k = 0; k < 6; ++k) A0[0][k] = k == 1 ? 1.0 : 0.0;
+        for (int k = 0; k < 6; ++k) rhs0[k] = G.v[0][k];
+        rhs0[0] = 0.0;
+        if (!solve6(A0, rhs0)) { report(I, 1 + 2 * stage, 3, (unsigned)R.gid); return; }
+        for (int k = 0; k < 6; ++k) u[0][k] = rhs0[k];
+        const double gi = P.gamma_i - 1.0, ge = P.gamma_e - 1.0, gr = P.gamma_r - 1.0;
+        const double gt = gi + ge + gr;
+        double row1[6] = {-gt * sqd(u[0][2]) / (6.0 * sqd(u[0][0])), 0.0, gt * u[0][2] / (6.0 * u[0][0]), -ge, -gi,
+                          -gr};
+        double A1[6][6], rhs1[6];
+        for (int i = 0; i < 6; ++i)
+            for (int k = 0; k < 6; ++k) A1[i][k] = G.L[i][k];
+        for (int k = 0; k < 6; ++k) A1[0][k] = row1[k];
+        for (int k = 0; k < 6; ++k) rhs1[k] = G.v[1][k];
+        rhs1[0] = 0.0;
+        if (!solve6(A1, rhs1)) { report(I, 1 + 2 * stage, 3, (unsigned)R.gid); return; }
+        for (int k = 0; k < 6; ++k) u[1][k] = rhs1[k];
+        for (int k = 2; k <= 4; ++k) matvec_cols(G.R, G.v[k], u[k]);
+    } else if (R.kind == BC_OUTFLOW) {
+        // bc1.rs:760-828
+        const DevBC& bc = I.bcs[R.bc];
+        matvec_cols(G.R, G.v[0], u[0]);
+        double rho0 = u[0][0];
+        double un0 = u[0][1] / rho0, ut0 = u[0][2] / rho0;
+        double w2 = un0 * un0 + ut0 * ut0;
+        double ee1 = u[0][3] / rho0 - w2 / 6.0, ei1 = u[0][4] / rho0 - w2 / 6.0, er1 = u[0][5] / rho0 - w2 / 6.0;
+        double ge = P.gamma_e - 1.0, gi = P.gamma_i - 1.0, gr = P.gamma_r - 1.0;
+        double p0 = rho0 * (ge * ee1 + gi * ei1 + gr * er1);
+        double a2 = P.gamma_e * ge * ee1 + P.gamma_i * gi * ei1 + P.gamma_r * gr * er1;
+        double a = sqrt(a2);
+        double lambda1 = un0 - a;
+        double rhs1[6];
+        for (int k = 0; k < 6; ++k) rhs1[k] = G.v[1][k];
+        if (lambda1 < 0.0) {
+            double m_local = fabs(un0 / a);
+            double l1 = bc.sigma * (1.0 - sqd(m_local)) * a / bc.l_domain * (p0 - bc.p_inf);
+            rhs1[0] = l1 / lambda1;
+        }
+        matvec_cols(G.R, rhs1, u[1]);
+        for (int k = 2; k <= 4; ++k) matvec_cols(G.R, G.v[k], u[k]);
+    } else {
+        // FarField, bc1.rs:829-924
+        const DevBC& bc = I.bcs[R.bc];
+        const double* ui = bc.state;
+        double uinf[6] = {ui[0], ui[1] * R.nx + ui[2] * R.ny, -ui[1] * R.ny + ui[2] * R.nx, ui[3], ui[4], ui[5]};
+        double vinf[6];
+        matvec_rows(G.L, uinf, vinf);
+        double rk[6];
+        for (int k = 0; k < 6; ++k) rk[k] = G.lam[k] < 0.0 ? vinf[k] : G.v[0][k];
+        matvec_cols(G.R, rk, u[0]);
+        for (int kk = 1; kk <= 4; ++kk) {
+            for (int k = 0; k < 6; ++k) rk[k] = G.lam[k] < 0.0 ? 0.0 : G.v[kk][k];
+            matvec_cols(G.R, rk, u[kk]);
+        }
+    }
+    // Taylor expansion + rotation back (bc1.rs:733-755)
+    double gv[6];
+    for (int k = 0; k < 6; ++k) gv[k] = u[0][k];
+    double coef = 1.0;
+    for (int k = 1; k <= 4; ++k) {
+        coef *= R.dist / (double)k;
+        for (int cc = 0; cc < 6; ++cc) gv[cc] = gv[cc] + coef * u[k][cc];
+    }
+    double mn = gv[1], mt = gv[2];
+    double out[6] = {gv[0], mn * R.nx - mt * R.ny, mn * R.ny + mt * R.nx, gv[3], gv[4], gv[5]};
+    bool fin = true;
+    double* wbuf = const_cast<double*>(buf);
+    for (int k = 0; k < 6; ++k) {
+        fin = fin && isfinite(out[k]);
+        wbuf[k * plane + R.node] = out[k];
+    }
+    if (!fin) report(I, 1 + 2 * stage, 2, (unsigned)R.gid);
+}
+
+// ------------------------------------------------------------------ fluxes
+// One thread per interface. The characteristic loop is outermost: for each
+// characteristic field c the thread forms row c of L, the six projected
+// fluxes/states, the two WENO5 reconstructions and accumulates column c of
+// R, which keeps the reference's association of R.(f+ + f-) (weno.rs:685-802).
+template <int DIR>
+__device__ __forceinline__ void face_flux(const Inst& I, const double* __restrict__ buf, int i, int j,
+                                          double* __restrict__ fout, long long fplane, long long fidx,
+                                          double* __restrict__ dout) {
+    const DevParams& P = I.P;
+    const long long plane = I.plane;
+    double s[6][6], F[6][6];
+    Prim d2, d3;
+#pragma unroll
+    for (int p = 0; p < 6; ++p) {
+        long long n = DIR == 0 ? node_of(I, i - 3 + p, j) : node_of(I, i, j - 3 + p);
+        load6(buf, plane, n, s[p]);
+        Prim d = prim_from_state(s[p], P);
+        phys_flux<DIR>(s[p], d, F[p]);
+        if (p == 2) d2 = d;
+        if (p == 3) d3 = d;
+    }
+    Roe q = roe_average(s[3][0], d3, s[2][0], d2, P);
+    double out[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+        double Lc[6], Rc[6], lam;
+        l_row<DIR>(c, q, P, Lc);
+        r_col<DIR>(c, q, P, Rc, lam);
+        double a = fabs(lam);
+        double fp[6], fm[6];
+#pragma unroll
+        for (int p = 0; p < 6; ++p) {
+            double cf = Lc[0] * F[p][0] + Lc[1] * F[p][1] + Lc[2] * F[p][2] + Lc[3] * F[p][3] + Lc[4] * F[p][4] +
+                        Lc[5] * F[p][5];
+            double cs = Lc[0] * s[p][0] + Lc[1] * s[p][1] + Lc[2] * s[p][2] + Lc[3] * s[p][3] + Lc[4] * s[p][4] +
+                        Lc[5] * s[p][5];
+            fp[p] = 0.5 * (cf + a * cs);
+            fm[p] = 0.5 * (cf - a * cs);
+        }
+        double g = weno5(fp[0], fp[1], fp[2], fp[3], fp[4], P.eps) + weno5(fm[5], fm[4], fm[3], fm[2], fm[1], P.eps);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) out[k] = c == 0 ? Rc[k] * g : out[k] + Rc[k] * g;
+    }
+#pragma unroll
+    for (int k = 0; k < 6; ++k) fout[k * fplane + fidx] = out[k];
+    if (dout) {
+        // diffusion.rs:27-50 on the same six points
+        double te[6], ti[6], tr[6];
+#pragma unroll
+        for (int p = 0; p < 6; ++p) temps_from_state(s[p], P, te[p], ti[p], tr[p]);
+        double ee_t = P.kappa_e * (2.0 * te[5] - 25.0 * te[4] + 245.0 * te[3] - 245.0 * te[2] + 25.0 * te[1] - 2.0 * te[0]);
+        double ei_t = P.kappa_i * (2.0 * ti[5] - 25.0 * ti[4] + 245.0 * ti[3] - 245.0 * ti[2] + 25.0 * ti[1] - 2.0 * ti[0]);
+        double er_t = P.kappa_r * (2.0 * pow4d(tr[5]) - 25.0 * pow4d(tr[4]) + 245.0 * pow4d(tr[3]) -
+                                   245.0 * pow4d(tr[2]) + 25.0 * pow4d(tr[1]) - 2.0 * pow4d(tr[0]));
+        dout[fidx] = ee_t / 180.0;
+        dout[fplane + fidx] = ei_t / 180.0;
+        dout[2 * fplane + fidx] = er_t / 180.0;
+    }
+}
+
+__global__ void __launch_bounds__(128) k_flux(const Inst* __restrict__ insts, const Tile* __restrict__ tx, int ntx,
+                                              const Tile* __restrict__ ty, int nty, int stage) {
+    const int b = blockIdx.x;
+    if (b < ntx) {
+        const Tile t = tx[b];
+        const Inst& I = insts[t.inst];
+        const int j = t.j0 + threadIdx.x;
+        if (j >= I.ny || has_error(I)) return;
+        const int i = t.i;
+        if (!(I.mask[node_of(I, i, j)] | I.mask[node_of(I, i - 1, j)])) {
+            const long long fp = (long long)(I.nx + 1) * I.ny, fi = (long long)i * I.ny + j;
+#pragma unroll
+            for (int k = 0; k < 6; ++k) I.fx[k * fp + fi] = 0.0;
+            return;
+        }
+        const long long fp = (long long)(I.nx + 1) * I.ny;
+        face_flux<0>(I, stage_src(I, stage), i, j, I.fx, fp, (long long)i * I.ny + j, I.diffusion ? I.dfx : nullptr);
+    } else if (b < ntx + nty) {
+        const Tile t = ty[b - ntx];
+        const Inst& I = insts[t.inst];
+        const int j = t.j0 + threadIdx.x;
+        if (j > I.ny || has_error(I)) return;
+        const int i = t.i;
+        const long long fp = (long long)I.nx * (I.ny + 1), fi = (long long)i * (I.ny + 1) + j;
+        if (!(I.mask[node_of(I, i, j)] | I.mask[node_of(I, i, j - 1)])) {
+#pragma unroll
+            for (int k = 0; k < 6; ++k) I.fy[k * fp + fi] = 0.0;
+            return;
+        }
+        face_flux<1>(I, stage_src(I, stage), i, j, I.fy, fp, fi, I.diffusion ? I.dfy : nullptr);
+    }
+}
+
+// ------------------------------------------------------------------ rhs + stage
+// main.rs:251-304 cell RHS fused with main.rs:308-349 stage update.
+// mode 0: write rhs to `rhs_out` (6 planes of nx*ny, i*ny+j) for l();
+// mode 1: stage update with admissibility check (main.rs:22-33).
+__device__ __forceinline__ void prim4(const double* __restrict__ buf, long long plane, long long n, const DevParams& P,
+                                      int dir, double& pe, double& pi, double& pr, double& vel) {
+    double s[6];
+    load6(buf, plane, n, s);
+    Prim d = prim_from_state(s, P);
+    pe = d.pe; pi = d.pi; pr = d.pr;
+    vel = dir == 0 ? d.u : d.v;
+}
+
+__global__ void __launch_bounds__(128) k_rhs_stage(const Inst* __restrict__ insts, const Tile* __restrict__ tiles,
+                                                   int nt, int stage, int mode, double* __restrict__ rhs_out) {
+    if (blockIdx.x >= nt) return;
+    const Tile t = tiles[blockIdx.x];
+    const Inst& I = insts[t.inst];
+    const int i = t.i, j = t.j0 + threadIdx.x;
+    if (j >= I.ny || has_error(I)) return;
+    const long long n = node_of(I, i, j);
+    if (!I.mask[n]) return;
+    const DevParams& P = I.P;
+    const long long plane = I.plane;
+    const double* __restrict__ src = stage_src(I, stage);
+    const double dx = I.dx, dy = I.dy;
+    const long long fpx = (long long)(I.nx + 1) * I.ny, fix = (long long)i * I.ny + j;
+    const long long fpy = (long long)I.nx * (I.ny + 1), fiy = (long long)i * (I.ny + 1) + j;
+    double rhs[6];
+    const double sx = 1.0 / dx, sy = 1.0 / dy;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+        double fl = I.fx[c * fpx + fix], fr = I.fx[c * fpx + fix + I.ny];
+        double fb = I.fy[c * fpy + fiy], ft = I.fy[c * fpy + fiy + 1];
+        rhs[c] = -(fr - fl) * sx + -(ft - fb) * sy;
+    }
+    double pe[9], pi[9], pr[9], vel[9], ncx[3], ncy[3];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) prim4(src, plane, node_of(I, i - 4 + q, j), P, 0, pe[q], pi[q], pr[q], vel[q]);
+    noncon9(pe, pi, pr, vel, dx, ncx);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) prim4(src, plane, node_of(I, i, j - 4 + q), P, 1, pe[q], pi[q], pr[q], vel[q]);
+    noncon9(pe, pi, pr, vel, dy, ncy);
+    double add[3] = {ncx[0], ncx[1], ncx[2]};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) rhs[3 + k] = rhs[3 + k] + add[k] + ncy[k];
+    if (I.source) {
+        // source.rs:7-21
+        double s[6];
+        load6(src, plane, n, s);
+        double te, ti, tr;
+        temps_from_state(s, P, te, ti, tr);
+        double so[3] = {-P.omega_ei * (te - ti) - P.omega_er * (pow4d(te) - pow4d(tr)), P.omega_ei * (te - ti),
+                        P.omega_er * (pow4d(te) - pow4d(tr))};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) rhs[3 + k] = rhs[3 + k] + so[k];
+    }
+    if (I.diffusion) {
+        const double cx = -1.0 / (dx * dx), cy = -1.0 / (dy * dy);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            double a = I.dfx[k * fpx + fix], b = I.dfx[k * fpx + fix + I.ny];
+            double c2 = I.dfy[k * fpy + fiy], d2 = I.dfy[k * fpy + fiy + 1];
+            rhs[3 + k] = rhs[3 + k] + ((-(b - a) * cx) + (-(d2 - c2) * cy));
+        }
+    }
+    if (mode == 0) {
+        const long long ln = (long long)i * I.ny + j, lp = (long long)I.nx * I.ny;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) rhs_out[c * lp + ln] = rhs[c];
+        return;
+    }
+    const DevScalars& sc = *I.sc;
+    double v[6];
+    if (stage == 0) {
+        const double coef = sc.coef[0];
+#pragma unroll
+        for (int c = 0; c < 6; ++c) v[c] = I.U[c * plane + n] + rhs[c] * coef;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) I.A[c * plane + n] = v[c];
+    } else if (stage == 1) {
+        const double coef = sc.coef[1];
+#pragma unroll
+        for (int c = 0; c < 6; ++c) v[c] = I.U[c * plane + n] * 0.75 + I.A[c * plane + n] * 0.25 + rhs[c] * coef;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) I.B[c * plane + n] = v[c];
+    } else {
+        const double coef = sc.coef[2];
+        const double wb = 1.0 / 3.0, wa = 2.0 / 3.0;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) v[c] = I.U[c * plane + n] * wb + I.B[c * plane + n] * wa + rhs[c] * coef;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) I.U[c * plane + n] = v[c];
+    }
+    bool ok = isfinite(v[0]) && isfinite(v[1]) && isfinite(v[2]) && isfinite(v[3]) && isfinite(v[4]) &&
+              isfinite(v[5]) && v[0] > 0.0;
+    if (ok) {
+        double ux = v[1] / v[0], uy = v[2] / v[0];
+        double k = (ux * ux + uy * uy) / 6.0;
+        ok = !(v[3] / v[0] - k <= 0.0 || v[4] / v[0] - k <= 0.0 || v[5] / v[0] - k <= 0.0);
+    }
+    if (!ok) report(I, 2 + 2 * stage, 1, (unsigned)((long long)i * I.ny + j));
+}
+
+// ------------------------------------------------------------------ dt
+// Orderable 64-bit key of a double (total order, NaN excluded by the caller).
+__device__ __forceinline__ unsigned long long dkey(double x) {
+    unsigned long long b = (unsigned long long)__double_as_longlong(x);
+    return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double dkey_inv(unsigned long long k) {
+    unsigned long long b = (k & 0x8000000000000000ull) ? (k & ~0x8000000000000000ull) : ~k;
+    return __longlong_as_double((long long)b);
+}
+
+// mode 0: dt_cfl only; mode 1: start of a step (dt = cfl_factor * dt_cfl,
+// clipped to t_final, stage times and coefficients, main.rs:460-464).
+__device__ void finalize_step(const Inst& I, double dt_cfl, int mode) {
+    DevScalars& sc = *I.sc;
+    if (mode == 1) {
+        sc.step = sc.steps_started;
+        sc.steps_started += 1;
+        double t = sc.t_after;
+        double dt = sc.cfl_factor * dt_cfl;
+        if (t + dt > sc.t_final) dt = sc.t_final - t;
+        if (!(dt > 0.0)) report(I, 0, 9, 0u);
+        sc.t = t;
+        sc.dt = dt;
+        sc.t_stage[0] = t;
+        sc.t_stage[1] = t + dt;
+        sc.t_stage[2] = t + 0.5 * dt;
+        sc.t_after = t + dt;
+        sc.coef[0] = dt;
+        sc.coef[1] = dt / 4.0;
+        sc.coef[2] = 2.0 * dt / 3.0;
+    }
+}
+
+__global__ void __launch_bounds__(128) k_dt(const Inst* __restrict__ insts, const Tile* __restrict__ tiles, int nt,
+                                            int mode) {
+    __shared__ double red[4];
+    __shared__ bool last;
+    if (blockIdx.x >= nt) return;
+    const Tile t = tiles[blockIdx.x];
+    const Inst& I = insts[t.inst];
+    const int i = t.i, j = t.j0 + threadIdx.x;
+    double m = INFINITY;
+    if (j < I.ny) {
+        const long long n = node_of(I, i, j);
+        if (I.mask[n]) {
+            double s[6];
+            load6(I.U, I.plane, n, s);
+            double d = local_dt(s, I.dx, I.dy, I.P);
+            m = fmin(m, d);
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double bm = fmin(fmin(red[0], red[1]), fmin(red[2], red[3]));
+        if (!isnan(bm)) atomicMin(&I.sc->dt_cfl_bits, dkey(bm));
+        __threadfence();
+        unsigned int done = atomicAdd(&I.sc->counter, 1u);
+        last = done == (unsigned)I.n_tiles_dt - 1u;
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        unsigned long long k = atomicAdd(&I.sc->dt_cfl_bits, 0ull);
+        double dt_cfl = dkey_inv(k);
+        I.sc->dt_cfl_bits = dkey(INFINITY);
+        I.sc->counter = 0u;
+        I.sc->dt_cfl = dt_cfl;
+        finalize_step(I, dt_cfl, mode);
+    }
+}
+
+// A step with a caller-given dt (rk3_ssp(dt), main.rs:351-373)
+__global__ void k_set_dt(const Inst* __restrict__ insts, int n_inst, double dt) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n_inst) return;
+    DevScalars& sc = *insts[k].sc;
+    sc.step = sc.steps_started;
+    sc.steps_started += 1;
+    double t = sc.t_after;
+    sc.t = t;
+    sc.dt = dt;
+    sc.t_stage[0] = t;
+    sc.t_stage[1] = t + dt;
+    sc.t_stage[2] = t + 0.5 * dt;
+    sc.t_after = t + dt;
+    sc.coef[0] = dt;
+    sc.coef[1] = dt / 4.0;
+    sc.coef[2] = 2.0 * dt / 3.0;
+}
+
+// ------------------------------------------------------------------ layout
+// AoS (i*ny+j, 6 doubles) <-> padded SoA planes of buffer U, fluid cells only.
+__global__ void k_scatter(const Inst* __restrict__ insts, int inst, const double* __restrict__ aos, double time) {
+    const Inst& I = insts[inst];
+    long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (l == 0) {
+        I.sc->t_after = time;
+        I.sc->t = time;
+    }
+    if (l >= (long long)I.nx * I.ny) return;
+    int i = (int)(l / I.ny), j = (int)(l % I.ny);
+    long long n = node_of(I, i, j);
+    if (!I.mask[n]) return;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) I.U[c * I.plane + n] = aos[l * 6 + c];
+}
+
+__global__ void k_gather(const Inst* __restrict__ insts, int inst, double* __restrict__ aos) {
+    const Inst& I = insts[inst];
+    long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= (long long)I.nx * I.ny) return;
+    int i = (int)(l / I.ny), j = (int)(l % I.ny);
+    long long n = node_of(I, i, j);
+    bool f = I.mask[n] != 0;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) aos[l * 6 + c] = f ? I.U[c * I.plane + n] : 0.0;
+}
+
+// planes (6 x nx*ny) -> AoS, for rh3t_l's rhs
+__global__ void k_planes_to_aos(const double* __restrict__ planes, long long n, double* __restrict__ aos) {
+    long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= n) return;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) aos[l * 6 + c] = planes[c * n + l];
+}
+
+// ghost values of stage buffer U -> (n_ghosts x 6)
+__global__ void k_ghost_values(const Inst* __restrict__ insts, const GhostRec* __restrict__ recs, int n,
+                               double* __restrict__ out) {
+    int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    const GhostRec R = recs[g];
+    const Inst& I = insts[R.inst];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) out[(long long)g * 6 + c] = I.U[c * I.plane + R.node];
+}
+
+// ------------------------------------------------------------------ host launchers
+void launch_ghosts(cudaStream_t s, const Inst* insts, const GhostRec* recs, int n, const int32_t* hst,
+                   const double* hs, const double* hw, const double* hd, int stage) {
+    if (n <= 0) return;
+    dim3 blk(6, 32);
+    k_ghosts<<<(n + 31) / 32, blk, 0, s>>>(insts, recs, n, hst, hs, hw, hd, stage);
+}
+void launch_flux(cudaStream_t s, const Inst* insts, const Tile* tx, int ntx, const Tile* ty, int nty, int stage) {
+    if (ntx + nty <= 0) return;
+    k_flux<<<ntx + nty, 128, 0, s>>>(insts, tx, ntx, ty, nty, stage);
+}
+void launch_rhs_stage(cudaStream_t s, const Inst* insts, const Tile* tc, int nt, int stage, int mode, double* rhs) {
+    if (nt <= 0) return;
+    k_rhs_stage<<<nt, 128, 0, s>>>(insts, tc, nt, stage, mode, rhs);
+}
+void launch_dt(cudaStream_t s, const Inst* insts, const Tile* tc, int nt, int mode) {
+    if (nt <= 0) return;
+    k_dt<<<nt, 128, 0, s>>>(insts, tc, nt, mode);
+}
+void launch_set_dt(cudaStream_t s, const Inst* insts, int n_inst, double dt) {
+    k_set_dt<<<(n_inst + 127) / 128, 128, 0, s>>>(insts, n_inst, dt);
+}
+void launch_scatter(cudaStream_t s, const Inst* insts, int inst, long long ncell, const double* aos, double time) {
+    k_scatter<<<(unsigned)((ncell + 255) / 256), 256, 0, s>>>(insts, inst, aos, time);
+}
+void launch_gather(cudaStream_t s, const Inst* insts, int inst, long long ncell, double* aos) {
+    k_gather<<<(unsigned)((ncell + 255) / 256), 256, 0, s>>>(insts, inst, aos);
+}
+void launch_planes_to_aos(cudaStream_t s, const double* planes, long long n, double* aos) {
+    k_planes_to_aos<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(planes, n, aos);
+}
+void launch_ghost_values(cudaStream_t s, const Inst* insts, const GhostRec* recs, int n, double* out) {
+    if (n <= 0) return;
+    k_ghost_values<<<(n + 127) / 128, 128, 0, s>>>(insts, recs, n, out);
+}
+
+} // namespace rh3t

@@ -1,0 +1,287 @@
+// Device-side pointwise physics of the 3T_RH operator, FP64.
+//
+// Each function restates the reference expression with the same association
+// order (colinhu123/3T_RH src/state.rs, weno.rs, noncon.rs, diffusion.rs,
+// source.rs, dt.rs); the only arithmetic freedom taken is the compiler's
+// mul+add -> FMA contraction (disabled in the RH3T_EXACT build).
+#pragma once
+#include "rh3t_dev.h"
+
+namespace rh3t {
+
+__device__ __forceinline__ double sqd(double x) { return x * x; }
+__device__ __forceinline__ double pow4d(double x) { return (x * x) * (x * x); }
+
+// Subset of state.rs:245-276 Derived::from_state needed by fluxes, L/R and noncon.
+struct Prim {
+    double u, v, e_e, e_i, e_r, pe, pi, pr;
+};
+
+__device__ __forceinline__ Prim prim_from_state(const double s[6], const DevParams& P) {
+    Prim d;
+    d.u = s[1] / s[0];
+    d.v = s[2] / s[0];
+    double w2 = sqd(d.u) + sqd(d.v);
+    d.e_e = s[3] / s[0] - w2 / 6.0;
+    d.e_i = s[4] / s[0] - w2 / 6.0;
+    d.e_r = s[5] / s[0] - w2 / 6.0;
+    d.pe = (P.gamma_e - 1.0) * (s[3] - s[0] * w2 / 6.0);
+    d.pi = (P.gamma_i - 1.0) * (s[4] - s[0] * w2 / 6.0);
+    d.pr = (P.gamma_r - 1.0) * (s[5] - s[0] * w2 / 6.0);
+    return d;
+}
+
+// state.rs:245-276 te, ti, tr (diffusion and source only)
+__device__ __forceinline__ void temps_from_state(const double s[6], const DevParams& P, double& te, double& ti,
+                                                 double& tr) {
+    double u = s[1] / s[0], v = s[2] / s[0];
+    double w2 = sqd(u) + sqd(v);
+    te = s[3] / (s[0] * P.cve) - w2 / (6.0 * P.cve);
+    ti = s[4] / (s[0] * P.cvi) - w2 / (6.0 * P.cvi);
+    double er_term = s[5] / s[0] - w2 / 6.0;
+    tr = pow(er_term * s[0] / P.a_rad, 0.25);
+}
+
+// state.rs:56-85 flux_from_derived
+template <int DIR>
+__device__ __forceinline__ void phys_flux(const double s[6], const Prim& d, double f[6]) {
+    double u = d.u, v = d.v;
+    double p = d.pe + d.pi + d.pr;
+    double rho = s[0];
+    if (DIR == 0) {
+        f[0] = rho * u; f[1] = rho * u * u + p; f[2] = rho * u * v;
+        f[3] = (s[3] + d.pe) * u; f[4] = (s[4] + d.pi) * u; f[5] = (s[5] + d.pr) * u;
+    } else {
+        f[0] = rho * v; f[1] = rho * u * v; f[2] = rho * v * v + p;
+        f[3] = (s[3] + d.pe) * v; f[4] = (s[4] + d.pi) * v; f[5] = (s[5] + d.pr) * v;
+    }
+}
+
+// Roe (sqrt(rho)-weighted) averages shared by weno.rs:28-78 build_l_plain and
+// weno.rs:484-516 build_r_plain (state1 = points[3], state2 = points[2]).
+struct Roe {
+    double u, v, w2, ee, ei, er, cs2, cs, he, hi, hr, b, den;
+};
+
+__device__ __forceinline__ Roe roe_average(double rho_s1, const Prim& d3, double rho_s2, const Prim& d2,
+                                           const DevParams& P) {
+    Roe q;
+    double rho1 = sqrt(rho_s1), rho2 = sqrt(rho_s2);
+    double rho_sum = rho1 + rho2;
+    q.u = (d3.u * rho1 + d2.u * rho2) / rho_sum;
+    q.v = (d3.v * rho1 + d2.v * rho2) / rho_sum;
+    q.w2 = sqd(q.u) + sqd(q.v);
+    q.ee = (d3.e_e * rho1 + d2.e_e * rho2) / rho_sum;
+    q.ei = (d3.e_i * rho1 + d2.e_i * rho2) / rho_sum;
+    q.er = (d3.e_r * rho1 + d2.e_r * rho2) / rho_sum;
+    const double GE = P.gamma_e, GI = P.gamma_i, GR = P.gamma_r;
+    const double gi = GI - 1.0, ge = GE - 1.0, gr = GR - 1.0;
+    const double gt = gi + ge + gr;
+    q.cs2 = GE * ge * q.ee + GI * gi * q.ei + GR * gr * q.er;
+    q.cs = sqrt(q.cs2);
+    q.he = 6.0 * gi * gr * (GI * q.ei - GR * q.er) + GE * gt * q.ee * q.w2;
+    q.hi = 6.0 * ge * gr * (GR * q.er - GE * q.ee) + GI * gt * q.ei * q.w2;
+    q.hr = 6.0 * ge * gi * (GE * q.ee - GI * q.ei) + GR * gt * q.er * q.w2;
+    q.b = gt * (36.0 * ge * gi * gr + gt * sqd(q.w2)) * q.cs2;
+    q.den = 12.0 * q.cs2;
+    return q;
+}
+
+// Row `row` of the left eigenvector matrix (weno.rs:79-458). DIR 0: rows
+// [u-c, e, i, r, transverse, u+c]; DIR 1: [v-c, transverse, e, i, r, v+c].
+template <int DIR>
+__device__ __forceinline__ void l_row(int row, const Roe& q, const DevParams& P, double L[6]) {
+    const double GE = P.gamma_e, GI = P.gamma_i, GR = P.gamma_r;
+    const double gi = GI - 1.0, ge = GE - 1.0, gr = GR - 1.0;
+    const double gt = gi + ge + gr;
+    const double u = q.u, v = q.v, w2 = q.w2, cs = q.cs, cs2 = q.cs2, b = q.b, den = q.den;
+    // map to a mode: 0 acoustic-, 1 transverse, 2 electron, 3 ion, 4 radiation, 5 acoustic+
+    int mode;
+    if (DIR == 0) {
+        const int m[6] = {0, 2, 3, 4, 1, 5};
+        mode = m[row];
+    } else {
+        const int m[6] = {0, 1, 2, 3, 4, 5};
+        mode = m[row];
+    }
+    if (mode == 0 || mode == 5) {
+        const double sgn = mode == 0 ? 1.0 : -1.0;
+        if (DIR == 0) {
+            L[0] = mode == 0 ? (gt * w2 + 6.0 * u * cs) / den : (gt * w2 - 6.0 * u * cs) / den;
+            L[1] = mode == 0 ? (-2.0 * gt * u - 6.0 * cs) / den : (-2.0 * gt * u + 6.0 * cs) / den;
+            L[2] = (-2.0 * gt * v) / den;
+        } else {
+            L[0] = mode == 0 ? (gt * w2 + 6.0 * v * cs) / den : (gt * w2 - 6.0 * v * cs) / den;
+            L[1] = (-2.0 * gt * u) / den;
+            L[2] = mode == 0 ? (-2.0 * gt * v - 6.0 * cs) / den : (-2.0 * gt * v + 6.0 * cs) / den;
+        }
+        (void)sgn;
+        L[3] = 6.0 * ge / den;
+        L[4] = 6.0 * gi / den;
+        L[5] = 6.0 * gr / den;
+    } else if (mode == 1) {
+        if (DIR == 0) { L[0] = -v; L[1] = 0.0; L[2] = 1.0; }
+        else { L[0] = -u; L[1] = 1.0; L[2] = 0.0; }
+        L[3] = 0.0; L[4] = 0.0; L[5] = 0.0;
+    } else if (mode == 2) {
+        const double he = q.he;
+        L[0] = ge / gt - ge * w2 / (6.0 * cs2) - ge * gt * w2 / b * (he - cs2 * w2);
+        L[1] = ge * u / (3.0 * cs2) + 2.0 * ge * gt * u / b * (he - cs2 * w2);
+        L[2] = ge * v / (3.0 * cs2) + 2.0 * ge * gt * v / b * (he - cs2 * w2);
+        L[3] = -sqd(ge) / (gt * cs2) - 6.0 * ge / b * (ge * he - gt * cs2 * w2);
+        L[4] = -ge * gi / (gt * cs2) - 6.0 * ge * gi / b * (he - 6.0 * gr * cs2);
+        L[5] = -ge * gr / (gt * cs2) - 6.0 * ge * gr / b * (he + 6.0 * gi * cs2);
+    } else if (mode == 3) {
+        const double hi = q.hi;
+        L[0] = gi / gt - gi * w2 / (6.0 * cs2) - gi * gt * w2 / b * (hi - cs2 * w2);
+        L[1] = gi * u / (3.0 * cs2) + 2.0 * gi * gt * u / b * (hi - cs2 * w2);
+        L[2] = gi * v / (3.0 * cs2) + 2.0 * gi * gt * v / b * (hi - cs2 * w2);
+        L[3] = -gi * ge / (gt * cs2) - 6.0 * gi * ge / b * (hi + 6.0 * gr * cs2);
+        L[4] = -sqd(gi) / (gt * cs2) - 6.0 * gi / b * (gi * hi - gt * cs2 * w2);
+        L[5] = -gi * gr / (gt * cs2) - 6.0 * gi * gr / b * (hi - 6.0 * ge * cs2);
+    } else {
+        const double hr = q.hr;
+        L[0] = gr / gt - gr * w2 / (6.0 * cs2) - gr * gt * w2 / b * (hr - cs2 * w2);
+        L[1] = gr * u / (3.0 * cs2) + 2.0 * gr * gt * u / b * (hr - cs2 * w2);
+        L[2] = gr * v / (3.0 * cs2) + 2.0 * gr * gt * v / b * (hr - cs2 * w2);
+        L[3] = -gr * ge / (gt * cs2) - 6.0 * gr * ge / b * (hr - 6.0 * gi * cs2);
+        L[4] = -gr * gi / (gt * cs2) - 6.0 * gr * gi / b * (hr + 6.0 * ge * cs2);
+        L[5] = -sqd(gr) / (gt * cs2) - 6.0 * gr / b * (gr * hr - gt * cs2 * w2);
+    }
+}
+
+// Column `col` of the right eigenvector matrix and eigenvalue (weno.rs:518-545).
+template <int DIR>
+__device__ __forceinline__ void r_col(int col, const Roe& q, const DevParams& P, double R[6], double& lam) {
+    const double GE = P.gamma_e, GI = P.gamma_i, GR = P.gamma_r;
+    const double gi = GI - 1.0, ge = GE - 1.0, gr = GR - 1.0;
+    const double gt = gi + ge + gr;
+    const double u = q.u, v = q.v, w2 = q.w2, cs = q.cs;
+    if (DIR == 0) {
+        switch (col) {
+        case 0:
+            R[0] = 1.0; R[1] = u - cs; R[2] = v;
+            R[3] = GE * q.ee + w2 / 6.0 - u * cs / 3.0;
+            R[4] = GI * q.ei + w2 / 6.0 - u * cs / 3.0;
+            R[5] = GR * q.er + w2 / 6.0 - u * cs / 3.0;
+            lam = u - cs; break;
+        case 1: R[0] = 1.0; R[1] = u; R[2] = v; R[3] = gt * w2 / (6.0 * ge); R[4] = gr; R[5] = -gi; lam = u; break;
+        case 2: R[0] = 1.0; R[1] = u; R[2] = v; R[3] = -gr; R[4] = gt * w2 / (6.0 * gi); R[5] = ge; lam = u; break;
+        case 3: R[0] = 1.0; R[1] = u; R[2] = v; R[3] = gi; R[4] = -ge; R[5] = gt * w2 / (6.0 * gr); lam = u; break;
+        case 4: R[0] = 0.0; R[1] = 0.0; R[2] = 1.0; R[3] = v / 3.0; R[4] = v / 3.0; R[5] = v / 3.0; lam = u; break;
+        default:
+            R[0] = 1.0; R[1] = u + cs; R[2] = v;
+            R[3] = GE * q.ee + w2 / 6.0 + u * cs / 3.0;
+            R[4] = GI * q.ei + w2 / 6.0 + u * cs / 3.0;
+            R[5] = GR * q.er + w2 / 6.0 + u * cs / 3.0;
+            lam = u + cs; break;
+        }
+    } else {
+        switch (col) {
+        case 0:
+            R[0] = 1.0; R[1] = u; R[2] = v - cs;
+            R[3] = GE * q.ee + w2 / 6.0 - v * cs / 3.0;
+            R[4] = GI * q.ei + w2 / 6.0 - v * cs / 3.0;
+            R[5] = GR * q.er + w2 / 6.0 - v * cs / 3.0;
+            lam = v - cs; break;
+        case 1: R[0] = 0.0; R[1] = 1.0; R[2] = 0.0; R[3] = u / 3.0; R[4] = u / 3.0; R[5] = u / 3.0; lam = v; break;
+        case 2: R[0] = 1.0; R[1] = u; R[2] = v; R[3] = gt * w2 / (6.0 * ge); R[4] = gr; R[5] = -gi; lam = v; break;
+        case 3: R[0] = 1.0; R[1] = u; R[2] = v; R[3] = -gr; R[4] = gt * w2 / (6.0 * gi); R[5] = ge; lam = v; break;
+        case 4: R[0] = 1.0; R[1] = u; R[2] = v; R[3] = gi; R[4] = -ge; R[5] = gt * w2 / (6.0 * gr); lam = v; break;
+        default:
+            R[0] = 1.0; R[1] = u; R[2] = v + cs;
+            R[3] = GE * q.ee + w2 / 6.0 + v * cs / 3.0;
+            R[4] = GI * q.ei + w2 / 6.0 + v * cs / 3.0;
+            R[5] = GR * q.er + w2 / 6.0 + v * cs / 3.0;
+            lam = v + cs; break;
+        }
+    }
+}
+
+// weno.rs:847-886 weno5 (WENO-JS, p = 2)
+__device__ __forceinline__ double weno5(double u0, double u1, double u2, double u3, double u4, double eps) {
+    double beta2 = 13.0 / 12.0 * sqd(u2 - 2.0 * u3 + u4) + 0.25 * sqd(3.0 * u2 - 4.0 * u3 + u4);
+    double beta1 = 13.0 / 12.0 * sqd(u1 - 2.0 * u2 + u3) + 0.25 * sqd(u1 - u3);
+    double beta0 = 13.0 / 12.0 * sqd(u0 - 2.0 * u1 + u2) + 0.25 * sqd(u0 - 4.0 * u1 + 3.0 * u2);
+    double a0 = 0.1 / sqd(eps + beta0);
+    double a1 = 0.6 / sqd(eps + beta1);
+    double a2 = 0.3 / sqd(eps + beta2);
+    double sum_o = a0 + a1 + a2;
+    double w0 = a0 / sum_o, w1 = a1 / sum_o, w2 = a2 / sum_o;
+    double p0 = u0 / 3.0 - 7.0 / 6.0 * u1 + 11.0 / 6.0 * u2;
+    double p1 = -u1 / 6.0 + 5.0 / 6.0 * u2 + u3 / 3.0;
+    double p2 = u2 / 3.0 + 5.0 / 6.0 * u3 - u4 / 6.0;
+    return w0 * p0 + w1 * p1 + w2 * p2;
+}
+
+// noncon.rs:49-57
+__device__ __forceinline__ double q_pulse7(double b0, double b1, double b2, double b3, double b4, double b5,
+                                           double b6) {
+    return -0.00714285714285723 * b0 + 0.0595238095238118 * b1 - 0.240476190476197 * b2 +
+           0.759523809523819 * b3 + 0.509523809523803 * b4 - 0.0904761904761891 * b5 +
+           0.00952380952380977 * b6;
+}
+
+// noncon.rs:259-285 one component of n_jump_pre on an 8-point window a[0..7]
+__device__ __forceinline__ double jump8(const double* a) {
+    return q_pulse7(a[7], a[6], a[5], a[4], a[3], a[2], a[1]) - q_pulse7(a[0], a[1], a[2], a[3], a[4], a[5], a[6]);
+}
+
+// noncon.rs:26-44
+__device__ __forceinline__ double d6(double qm3, double qm2, double qm1, double qp1, double qp2, double qp3,
+                                     double dx) {
+    return (qp3 - 9.0 * qp2 + 45.0 * qp1 - 45.0 * qm1 + 9.0 * qm2 - qm3) / (60.0 * dx);
+}
+
+// noncon.rs:288-332 nonconservative_direction_pre on a 9-point window
+// (pe, pi, pr, transport velocity vel per point, index 4 = cell).
+__device__ __forceinline__ void noncon9(const double pe[9], const double pi[9], const double pr[9],
+                                        const double vel[9], double ds, double out[3]) {
+    double v = vel[4];
+    double dpe = d6(pe[1], pe[2], pe[3], pe[5], pe[6], pe[7], ds);
+    double dpi = d6(pi[1], pi[2], pi[3], pi[5], pi[6], pi[7], ds);
+    double dpr = d6(pr[1], pr[2], pr[3], pr[5], pr[6], pr[7], ds);
+    double der_ee = 2.0 * dpe - dpi - dpr;
+    double der_ei = 2.0 * dpi - dpe - dpr;
+    double der_er = 2.0 * dpr - dpe - dpi;
+    double nee[9], nei[9], ner[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        nee[k] = 2.0 * pe[k] - pi[k] - pr[k];
+        nei[k] = 2.0 * pi[k] - pe[k] - pr[k];
+        ner[k] = 2.0 * pr[k] - pe[k] - pi[k];
+    }
+    double jm_ee = jump8(nee), jm_ei = jump8(nei), jm_er = jump8(ner);
+    double jp_ee = jump8(nee + 1), jp_ei = jump8(nei + 1), jp_er = jump8(ner + 1);
+    double coef_left = fmax(fmax(v, vel[3]), 0.0) / 3.0;
+    double coef_right = fmin(fmin(v, vel[5]), 0.0) / 3.0;
+    out[0] = v / 3.0 * der_ee + (coef_left * jm_ee + coef_right * jp_ee) / ds;
+    out[1] = v / 3.0 * der_ei + (coef_left * jm_ei + coef_right * jp_ei) / ds;
+    out[2] = v / 3.0 * der_er + (coef_left * jm_er + coef_right * jp_er) / ds;
+}
+
+// dt.rs:5-34 get_local_dt (same association order; CVE^3 = CVE*(CVE*CVE))
+__device__ __forceinline__ double local_dt(const double s[6], double dx, double dy, const DevParams& P) {
+    double u = s[1] / s[0], v = s[2] / s[0];
+    double ee = s[3] / s[0] - (sqd(u) + sqd(v)) / 6.0;
+    double ei = s[4] / s[0] - (sqd(u) + sqd(v)) / 6.0;
+    double er = s[5] / s[0] - (sqd(u) + sqd(v)) / 6.0;
+    const double GE = P.gamma_e, GI = P.gamma_i, GR = P.gamma_r, A = P.a_rad, CVE = P.cve, CVI = P.cvi;
+    const double OEI = P.omega_ei, OER = P.omega_er;
+    const double gi = GI - 1.0, ge = GE - 1.0, gr = GR - 1.0;
+    double cs = sqrt(GE * ge * ee + GI * gi * ei + GR * gr * er);
+    const double c4 = (CVE * CVE) * (CVE * CVE), c3 = CVE * (CVE * CVE);
+    double ee3 = ee * (ee * ee);
+    double t1 = A * OEI * c4 + A * OEI * c3 * CVI + 4.0 * A * OER * CVI * ee3 + OER * c4 * CVI * s[0];
+    double s1 = sqrt(sqd(t1) - 4.0 * A * OEI * OER * c4 * CVI * (4.0 * A * ee3 + c4 * s[0] + c3 * CVI * s[0]));
+    double s2 = -(A * OEI * c4 + A * OEI * c3 * CVI + 4.0 * A * OER * CVI * ee3 + OER * c4 * CVI * s[0]);
+    double sden = 2.0 * A * c4 * CVI * s[0];
+    double alpha1 = fabs((-s1 + s2) / sden);
+    double alpha2 = fabs((s1 + s2) / sden);
+    double sj = fmax(alpha1, alpha2);
+    double dj = fmax(fmax(P.kappa_e / (CVE * s[0]), P.kappa_i / (CVI * s[0])), P.kappa_r / A);
+    double vj = (fabs(u) + cs) / dx + 2.0 * dj / (sqd(dx) + sqd(dy)) + sj + (fabs(v) + cs) / dy;
+    return P.lambda / vj;
+}
+
+} // namespace rh3t

@@ -1,0 +1,107 @@
+// Device data layout of the rh3t solver (shared by host and device code).
+//
+// HBM layout of one solver instance:
+//   state buffers U, A, B: 6 component planes each, padded node grid
+//     (nx + 2*PAD) x nyp with nyp = round_up(ny + 2*PAD, 8); node (i, j)
+//     lives at (i + PAD) * nyp + (j + PAD), j fastest (the reference's i*ny+j
+//     order, padded). Ghost values are written into their own node position,
+//     so every stencil read is a direct load (the reference goes through the
+//     per-cell access table of ghost.rs:71-107 instead).
+//   x faces fx: 6 planes of (nx+1)*ny, face (i, j) = interface i-1/2 of row j
+//     at i*ny + j; y faces fy: 6 planes of nx*(ny+1), face (i, j) =
+//     interface j-1/2 of column i at i*(ny+1) + j (main.rs:45-67 keeps y
+//     faces as [j][i]; j fastest here for coalescing).
+//   diffusion faces dfx/dfy: 3 planes (ee, ei, er) of the same shapes.
+#pragma once
+#include <stdint.h>
+
+#define RH3T_PAD 4
+
+namespace rh3t {
+
+struct DevParams {
+    double gamma_e, gamma_i, gamma_r;
+    double cve, cvi, a_rad;
+    double kappa_e, kappa_i, kappa_r;
+    double omega_ei, omega_er;
+    double lambda, weno_q, eps;
+    double periodic_ly;
+};
+
+struct DevBC {
+    int32_t kind;
+    int32_t reserved;
+    double state[6];
+    double p_inf, sigma, l_domain;
+    double td_x0, td_speed;
+    double td_left[6], td_right[6];
+};
+
+enum BCKind {
+    BC_REFLECTIVE_WALL = 0, BC_WALL = 1, BC_PERIODIC = 2, BC_CONSTANT = 3,
+    BC_TIME_DEPENDENT = 4, BC_OUTFLOW = 5, BC_ZEROTH_ORDER = 6, BC_FAR_FIELD = 7
+};
+
+// one ghost node (ghost.rs:18-27 GhostInfo, with the static parts of the
+// cheap BCs resolved at set-up: the mirror / wrap source node)
+struct GhostRec {
+    int32_t inst;     // instance id
+    int32_t bc;       // index into the instance's BC table (outer sides, then inner)
+    int32_t kind;     // BC kind of that side
+    int32_t node;     // padded node index of the ghost (write target)
+    int32_t src;      // padded node index of the source node (cheap kinds) or nearest node (heavy)
+    int32_t heavy;    // slot in the heavy tables or -1
+    int32_t gid;      // ghost id within its instance
+    int32_t pad_;
+    double p0x, p0y, nx, ny, dist;
+    double pad2_[3];
+};
+
+// per-instance scalars kept on the device (one 128-byte line)
+struct DevScalars {
+    unsigned long long dt_cfl_bits; // running min of local dt (bit pattern of a positive double)
+    unsigned int counter;           // blocks finished in the dt reduction
+    unsigned int pad_;
+    double dt;                      // dt of the current step
+    double t;                       // time at the start of the current step
+    double t_stage[3];              // ghost times of the three stages (main.rs:362, 366)
+    double t_after;                 // time after the current step
+    double cfl_factor, t_final;
+    double coef[3];                 // stage rhs coefficients dt, dt/4, 2dt/3
+    double dt_cfl;                  // last reduced dt_cfl (calc_global_dt)
+    long long step;                 // index of the current step (error keys)
+    long long steps_started;
+};
+
+// error record: one 64-bit key, min over all reports (the earliest failure):
+// key = step << 40 | phase << 37 | code << 32 | index, phase = 2*stage (+1
+// for the stage update, 0 for the ghost update of that stage; 7 = dt).
+struct DevError {
+    unsigned long long key;         // ~0ull when clear
+};
+
+struct Inst {
+    int32_t nx, ny, nyp, n_tiles_dt;
+    long long plane;                // (nx + 2*PAD) * nyp
+    double dx, dy;
+    DevParams P;
+    int32_t diffusion, source;
+    double* U;
+    double* A;
+    double* B;
+    const uint8_t* mask;            // padded fluid mask, 1 = fluid
+    double* fx;
+    double* fy;
+    double* dfx;
+    double* dfy;
+    const DevBC* bcs;
+    DevScalars* sc;
+    DevError* err;
+};
+
+// work tile: 128 consecutive j at one i
+struct Tile {
+    int32_t inst, i, j0, pad_;
+};
+
+} // namespace rh3t

@@ -1,0 +1,211 @@
+/*
+ * rh3t.h — C ABI of the B200 implementation of the 3T_RH semi-discrete
+ * operator l() and its SSP-RK3 driver (colinhu123/3T_RH, src/main.rs).
+ *
+ * The reference exposes this path only as private Rust functions of a binary
+ * crate (main.rs:135 l, main.rs:351 rk3_ssp, main.rs:375 calc_global_dt,
+ * ghost.rs:199 GhostGrid::update_values_parallel). Each entry point below
+ * names the reference item it replaces. Plain pointers and sizes only.
+ *
+ * Layouts shared with the reference:
+ *   - a field value array is nx*ny records of 6 doubles
+ *     (rho, mom_x, mom_y, ee, ei, er) at linear index i*ny + j
+ *     (field1.rs:205-215, state.rs:18-25);
+ *   - a fluid mask is nx*ny bytes at the same linear index (field1.rs:112-122).
+ *
+ * Errors: every call returns an rh3t_status. The reference panics instead;
+ * rh3t_last_error() returns the record a caller needs to re-raise the
+ * reference's message (stage label, cell or ghost index).
+ *
+ * Threading: one context = one CUDA stream; a context must not be used from
+ * two threads at once (the reference's l() takes &mut GhostGrid / &mut Scratch).
+ */
+#ifndef RH3T_H
+#define RH3T_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RH3T_ABI_VERSION 1
+
+typedef enum {
+    RH3T_OK = 0,
+    RH3T_ERR_NONPHYSICAL_STATE = 1, /* main.rs:30-33 assert_admissible panic */
+    RH3T_ERR_NONFINITE_GHOST = 2,   /* ghost.rs:229-263 panic */
+    RH3T_ERR_SINGULAR_ILW = 3,      /* bc1.rs:467-469 solve6 panic */
+    RH3T_ERR_PERIODIC_WRAP = 4,     /* bc1.rs:594-604 panic */
+    RH3T_ERR_STENCIL_FIT = 5,       /* bc1.rs:1429-1434 / 1466-1471 panic */
+    RH3T_ERR_GEOMETRY = 6,          /* geometry.rs / ghost.rs build-time asserts */
+    RH3T_ERR_INVALID_ARGUMENT = 7,
+    RH3T_ERR_CUDA = 8,
+    RH3T_ERR_NONPOSITIVE_DT = 9,    /* main.rs:464 assert!(dt > 0.0) */
+    RH3T_ERR_NO_DEVICE = 10
+} rh3t_status;
+
+/* field1.rs:6-15 GridInfo: node-centred x = x0 + i*dx, y = y0 + j*dy */
+typedef struct {
+    int32_t nx, ny;
+    double dx, dy, x0, y0;
+} rh3t_grid;
+
+/* constant.rs:1-25 as runtime values (the reference's are compile-time
+ * constants); rh3t_default_params() returns the reference values.
+ * periodic_ly replaces the hardcoded ly = 0.5 of bc1.rs:577. */
+typedef struct {
+    double gamma_e, gamma_i, gamma_r;
+    double cve, cvi, a_rad;
+    double kappa_e, kappa_i, kappa_r;
+    double omega_ei, omega_er;
+    double lambda, weno_q, eps;
+    double periodic_ly;
+} rh3t_params;
+
+/* bc1.rs:17-28 BCType */
+typedef enum {
+    RH3T_BC_REFLECTIVE_WALL = 0,
+    RH3T_BC_WALL = 1,
+    RH3T_BC_PERIODIC = 2,
+    RH3T_BC_CONSTANT = 3,
+    RH3T_BC_TIME_DEPENDENT = 4,
+    RH3T_BC_OUTFLOW = 5,
+    RH3T_BC_ZEROTH_ORDER = 6,
+    RH3T_BC_FAR_FIELD = 7
+} rh3t_bc_kind;
+
+/* One BCType value. state: Constant / FarField state. p_inf, sigma, l_domain:
+ * Outflow. TimeDependent carries the one closure the reference uses
+ * (init.rs:61-65): state = P0.x <= td_x0 + td_speed*t ? td_left : td_right. */
+typedef struct {
+    int32_t kind;
+    int32_t reserved;
+    double state[6];
+    double p_inf, sigma, l_domain;
+    double td_x0, td_speed;
+    double td_left[6], td_right[6];
+} rh3t_bc;
+
+/* geometry.rs:661-673 ArcOverride with the arc given by its three points
+ * (geometry.rs:492-549 CircularArc::from_three_points). boundary: 0 outer, 1 inner. */
+typedef struct {
+    int32_t boundary;
+    int32_t side_start, side_end;
+    int32_t fluid_side; /* 0 Inside, 1 Outside */
+    double start[2], mid[2], end[2];
+} rh3t_arc;
+
+/* ghost.rs:18-46 GhostGrid::info + bc1.rs:50-57 GhostBC, as SoA arrays.
+ * Ghost g: idx[2g..2g+1] = (i, j); proj[5g..5g+4] = (P0.x, P0.y, n.x, n.y, D)
+ * (the FINAL projection, ghost.rs:428-456); pre[g] = slot in the GhostBC
+ * arrays or -1 (only Wall / Outflow / FarField ghosts have one).
+ * GhostBC slot k: nearest[2k..], stencil[55k..] (linear indices i*ny+j),
+ * s[979k..], w[225k..], d[5k..] with the offsets of bc1.rs:45-47. */
+typedef struct {
+    int32_t n_ghosts;
+    const int32_t* idx;
+    const int32_t* boundary;
+    const int32_t* side;
+    const double* proj;
+    const int32_t* pre;
+    int32_t n_heavy;
+    const int32_t* nearest;
+    const uint32_t* stencil;
+    const double* s;
+    const double* w;
+    const double* d;
+} rh3t_ghost_table;
+
+typedef struct {
+    int32_t code;     /* rh3t_status */
+    int32_t stage;    /* 1..3 for RK stage states ("RK1 state" ...), 0 otherwise */
+    int64_t step;     /* step of rh3t_advance in which it happened (0-based) */
+    int32_t i, j;     /* cell index (code 1) or ghost grid index (code 2, 3, 4) */
+    int32_t ghost;    /* ghost id (codes 2, 3, 4), else -1 */
+    char message[160];
+} rh3t_error;
+
+/* ------------------------------------------------------------------ */
+/* Host mirror of Field::new + GhostGrid::build (field1.rs:95-136,     */
+/* ghost.rs:50-118, bc1.rs:108-188). Pure host code.                  */
+/* ------------------------------------------------------------------ */
+typedef struct rh3t_geom rh3t_geom;
+
+/* outer_xy / inner_xy: polygon points (x, y) pairs; *_fluid_side 0 Inside,
+ * 1 Outside; one rh3t_bc per polygon side (side k spans point k -> k+1).
+ * Replaces Field::new (field1.rs:95-136) + the arc registration of
+ * init.rs:461-467. */
+int rh3t_geom_create(const rh3t_grid* grid, const rh3t_params* params,
+                     int32_t n_outer, const double* outer_xy, int32_t outer_fluid_side, const rh3t_bc* outer_bcs,
+                     int32_t n_inner, const double* inner_xy, int32_t inner_fluid_side, const rh3t_bc* inner_bcs,
+                     int32_t n_arcs, const rh3t_arc* arcs, rh3t_geom** out);
+/* field1.rs:112-122 fluid mask, nx*ny bytes */
+int rh3t_geom_fluid_mask(const rh3t_geom* g, uint8_t* out);
+/* ghost.rs:50-118 GhostGrid::build with ghost.rs:482-493 default offsets;
+ * n_threads <= 0 uses all host cores. */
+int rh3t_geom_build_ghosts(rh3t_geom* g, int32_t n_threads);
+/* view of the built tables (valid until rh3t_geom_destroy) */
+int rh3t_geom_ghost_table(const rh3t_geom* g, rh3t_ghost_table* view);
+/* ghost.rs:71-107 access table, nx*ny*17 u32 (0 for non-fluid cells) */
+int rh3t_geom_access_table(const rh3t_geom* g, uint32_t* out);
+/* last build error text (NUL-terminated) */
+const char* rh3t_geom_last_error(const rh3t_geom* g);
+void rh3t_geom_destroy(rh3t_geom* g);
+
+/* ------------------------------------------------------------------ */
+/* Device solver, one instance                                         */
+/* ------------------------------------------------------------------ */
+typedef struct rh3t_ctx rh3t_ctx;
+
+void rh3t_default_params(rh3t_params* out);
+
+/* Creates the device copy of a Field (grid, mask, BC lists) and its
+ * GhostGrid. All tables are copied; the caller keeps ownership.
+ * n_outer_bc / n_inner_bc: BC list lengths (field1.rs Field::bc_outer/bc_inner). */
+int rh3t_create(const rh3t_grid* grid, const rh3t_params* params, const uint8_t* fluid,
+                int32_t n_outer_bc, const rh3t_bc* outer_bcs, int32_t n_inner_bc, const rh3t_bc* inner_bcs,
+                const rh3t_ghost_table* ghosts, int32_t device, rh3t_ctx** out);
+
+/* Field::value host <-> device (values of non-fluid cells are ignored on
+ * upload and returned as 0 on download), plus Field::time. */
+int rh3t_upload_state(rh3t_ctx* ctx, const double* value, double time);
+int rh3t_download_state(rh3t_ctx* ctx, double* value, double* time);
+
+/* main.rs:135-305 l(): ghost update + fluxes + RHS of the resident state at
+ * the resident time. rhs: nx*ny*6 (zero on non-fluid cells) or NULL;
+ * ghost_values: n_ghosts*6 (ghost.rs GhostGrid::values) or NULL. */
+int rh3t_l(rh3t_ctx* ctx, double* rhs, double* ghost_values);
+
+/* main.rs:375-408 calc_global_dt of the resident state */
+int rh3t_calc_global_dt(rh3t_ctx* ctx, double* dt_cfl);
+
+/* main.rs:351-373 rk3_ssp with a caller-given dt, resident state */
+int rh3t_rk3_ssp(rh3t_ctx* ctx, double dt);
+
+/* main.rs:459-477 time loop body repeated nsteps times on the device:
+ * dt = cfl_factor * calc_global_dt, clipped to t_final (pass INFINITY for
+ * none), then rk3_ssp. dt stays on the device; use_graph != 0 replays one
+ * captured CUDA graph per step. */
+int rh3t_advance(rh3t_ctx* ctx, int32_t nsteps, double cfl_factor, double t_final, int32_t use_graph);
+
+/* Drop-in step with a host-owned Field::value (the reference's own loop
+ * body, main.rs:460-466): upload value, dt = cfl_factor * calc_global_dt,
+ * rk3_ssp, download value (in place). dt_out may be NULL. */
+int rh3t_step_host(rh3t_ctx* ctx, double* value, double* time, double cfl_factor, double* dt_out);
+
+/* dt of the last step of rh3t_advance / rh3t_step_host (host read) */
+int rh3t_last_dt(rh3t_ctx* ctx, double* dt);
+
+int rh3t_synchronize(rh3t_ctx* ctx);
+int rh3t_last_error(const rh3t_ctx* ctx, rh3t_error* out);
+/* number of kernels this context launched since creation (instrumentation) */
+int64_t rh3t_kernel_launches(const rh3t_ctx* ctx);
+/* the CUDA stream the context runs on (cudaStream_t) */
+void* rh3t_stream(const rh3t_ctx* ctx);
+void rh3t_destroy(rh3t_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
