@@ -415,6 +415,14 @@ class Solver:
         self._check(self.L.rh3t_step_host(self.h, value.ctypes.data, C.byref(t), float(cfl_factor), C.byref(dt)))
         return t.value, dt.value
 
+    def profile_steps(self, nsteps, cfl_factor=0.05):
+        """Eager steps with CUDA events around every launch: device ms and
+        launch counts per kernel class (ghosts, fluxes, rhs+stage, dt)."""
+        ms = np.zeros(4)
+        cnt = np.zeros(4, np.int64)
+        self._check(self.L.rh3t_profile_steps(self.h, int(nsteps), float(cfl_factor), ms.ctypes.data, cnt.ctypes.data))
+        return dict(zip(("ghosts", "flux", "rhs_stage", "dt"), zip(ms.tolist(), cnt.tolist())))
+
     def last_dt(self):
         d = C.c_double()
         self._check(self.L.rh3t_last_dt(self.h, C.byref(d)))
@@ -430,6 +438,16 @@ class Solver:
     @property
     def stream(self):
         return self.L.rh3t_stream(self.h)
+
+
+def fp64_peak_tflops(device=0):
+    """Measured DFMA throughput of the device (TFLOP/s)."""
+    L = _lib.load()
+    t = C.c_double()
+    rc = L.rh3t_fp64_peak(device, C.byref(t))
+    if rc:
+        raise RH3TError(rc, "fp64 peak probe failed")
+    return t.value
 
 
 # ------------------------------------------------------------------ main.rs functions

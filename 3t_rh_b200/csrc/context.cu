@@ -263,7 +263,7 @@ extern "C" int rh3t_create(const rh3t_grid* grid, const rh3t_params* params, con
     DA(c->d_ty, std::max(c->nty, 1));
     DA(c->d_tc, std::max(c->ntc, 1));
     DA(c->d_io, nx * ny * 6);
-    DA(c->d_io2, nx * ny * 6);
+    DA(c->d_io2, std::max((long long)nx * ny, (long long)ng) * 6); // rhs planes or ghost values
 #undef DA
     I.U = c->d_state; I.A = c->d_state + 6 * plane; I.B = c->d_state + 12 * plane;
     I.mask = c->d_mask;
@@ -511,6 +511,90 @@ extern "C" int rh3t_step_host(rh3t_ctx* c, double* value, double* time, double c
                               cudaMemcpyDeviceToHost, s));
     CK(c, cudaGetLastError());
     return fetch_error(c);
+}
+
+extern "C" int rh3t_profile_steps(rh3t_ctx* c, int32_t nsteps, double cfl_factor, double* ms_out,
+                                  int64_t* launches_out) {
+    if (!c || !ms_out || nsteps < 0) return RH3T_ERR_INVALID_ARGUMENT;
+    CK(c, cudaSetDevice(c->device));
+    int rc = set_step_params(c, cfl_factor, INFINITY);
+    if (rc) return rc;
+    cudaStream_t s = c->stream;
+    std::vector<cudaEvent_t> ev;
+    std::vector<int> cls;
+    auto mark = [&](int k) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        cudaEventRecord(e, s);
+        ev.push_back(e);
+        cls.push_back(k);
+    };
+    for (int n = 0; n < nsteps; ++n) {
+        mark(-1);
+        launch_dt(s, c->d_inst, c->d_tc, c->ntc, 1);
+        mark(3);
+        for (int st = 0; st < 3; ++st) {
+            launch_ghosts(s, c->d_inst, c->d_ghosts, c->n_ghosts, c->d_hst, c->d_hs, c->d_hw, c->d_hd, st);
+            mark(0);
+            launch_flux(s, c->d_inst, c->d_tx, c->ntx, c->d_ty, c->nty, st);
+            mark(1);
+            launch_rhs_stage(s, c->d_inst, c->d_tc, c->ntc, st, 1, nullptr);
+            mark(2);
+        }
+    }
+    c->launches += (long long)nsteps * launches_per_step(c);
+    CK(c, cudaGetLastError());
+    CK(c, cudaStreamSynchronize(s));
+    double acc[4] = {0, 0, 0, 0};
+    int64_t cnt[4] = {0, 0, 0, 0};
+    for (size_t k = 1; k < ev.size(); ++k) {
+        if (cls[k] < 0) continue;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ev[k - 1], ev[k]);
+        acc[cls[k]] += ms;
+        cnt[cls[k]] += 1;
+    }
+    for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    for (int k = 0; k < 4; ++k) ms_out[k] = acc[k];
+    if (launches_out)
+        for (int k = 0; k < 4; ++k) launches_out[k] = cnt[k];
+    return fetch_error(c);
+}
+
+extern "C" int rh3t_fp64_peak(int32_t device, double* tflops) {
+    if (!tflops) return RH3T_ERR_INVALID_ARGUMENT;
+    if (cudaSetDevice(device) != cudaSuccess) return RH3T_ERR_NO_DEVICE;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return RH3T_ERR_CUDA;
+    double* out = nullptr;
+    int blocks = prop.multiProcessorCount * 8;
+    if (cudaMalloc(&out, blocks * sizeof(double)) != cudaSuccess) return RH3T_ERR_CUDA;
+    cudaStream_t s;
+    cudaStreamCreate(&s);
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    const int iters = 1 << 16;
+    launch_dfma(s, blocks, out, iters / 16); // warm-up
+    double best = 0.0;
+    for (int rep = 0; rep < 5; ++rep) {
+        cudaEventRecord(a, s);
+        launch_dfma(s, blocks, out, iters);
+        cudaEventRecord(b, s);
+        cudaEventSynchronize(b);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        double flops = 2.0 * 8.0 * (double)iters * (double)blocks * 256.0;
+        if (ms > 0) best = std::max(best, flops / (ms * 1e-3) / 1e12);
+    }
+    cudaError_t e = cudaGetLastError();
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaStreamDestroy(s);
+    cudaFree(out);
+    if (e != cudaSuccess) return RH3T_ERR_CUDA;
+    *tflops = best;
+    return RH3T_OK;
 }
 
 extern "C" int rh3t_last_dt(rh3t_ctx* c, double* dt) {

@@ -642,7 +642,27 @@ __global__ void k_ghost_values(const Inst* __restrict__ insts, const GhostRec* _
     for (int c = 0; c < 6; ++c) out[(long long)g * 6 + c] = I.U[c * I.plane + R.node];
 }
 
+// ------------------------------------------------------------------ FP64 peak probe
+// 8 independent FMA chains per thread, values kept in [0.5, 2].
+__global__ void __launch_bounds__(256) k_dfma(double* out, int iters, double b, double c) {
+    double a[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a[k] = 1.0 + 1e-3 * (threadIdx.x + k);
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) a[k] = fma(a[k], b, c);
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s += a[k];
+    if (s == 12345.678) out[blockIdx.x] = s; // never true; keeps the loop live
+}
+
 // ------------------------------------------------------------------ host launchers
+void launch_dfma(cudaStream_t s, int blocks, double* out, int iters) {
+    k_dfma<<<blocks, 256, 0, s>>>(out, iters, 0.9999999, 1e-7);
+}
+
 void launch_ghosts(cudaStream_t s, const Inst* insts, const GhostRec* recs, int n, const int32_t* hst,
                    const double* hs, const double* hw, const double* hd, int stage) {
     if (n <= 0) return;

@@ -1,0 +1,283 @@
+"""Benchmark of the rh3t B200 solver: cell-updates/s of the SSP-RK3 step.
+
+A step is one SSP-RK3 step (main.rs:459-466: dt = 0.05 * calc_global_dt, then
+rk3_ssp) of one solver instance; a cell-update is one fluid node advanced by
+one step. Default workload: the reference's Mach-3 half-cylinder refined to
+h = 1/320 (961 x 3841 nodes, 3,525,896 fluid cells), FP64.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                  [--workload cyl961|cyl481|cyl121|planar] [--exact]
+
+--impl reference times the reference algorithm's CPU implementation (the
+oracle restatement, OpenMP on all host cores; the Rust reference cannot be
+built on this image) on the same workload and prints the same JSON line.
+Multi-GPU runs are independent replicas (one instance per GPU, no exchange):
+value = all ranks' cell-updates / max-over-ranks device time.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "cyl961": dict(kind="cylinder", h=1.0 / 320.0, name="half-cylinder Mach-3, 961x3841 nodes (h=1/320)"),
+    "cyl481": dict(kind="cylinder", h=1.0 / 160.0, name="half-cylinder Mach-3, 481x1921 nodes (h=1/160)"),
+    "cyl121": dict(kind="cylinder", h=1.0 / 40.0, name="half-cylinder Mach-3, 121x481 nodes (h=1/40)"),
+    "planar": dict(kind="planar", name="Mach-2 planar shock, 1024x8, y-periodic, diffusion+exchange on"),
+}
+PLANAR_PARAMS = dict(kappa_e=1e-3, kappa_i=1e-3, kappa_r=1e-3, omega_ei=1.0, omega_er=1.0, periodic_ly=0.03125)
+CFL = 0.05
+
+
+def make_field(rh, wl):
+    spec = WORKLOADS[wl]
+    if spec["kind"] == "cylinder":
+        return rh.cases.init_cylinder(h=spec["h"])
+    return rh.cases.planar_shock(params=rh.Params(**PLANAR_PARAMS))
+
+
+def make_oracle(O, wl):
+    spec = WORKLOADS[wl]
+    if spec["kind"] == "cylinder":
+        return O.Case.cylinder(h=spec["h"])
+    return O.Case.planar_shock(**PLANAR_PARAMS)
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 100 ms."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.t.join(timeout=2)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if len(r) > 5 + k and r[5 + k] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def cpu_baseline(O, wl, budget_s=20.0):
+    """The oracle (OpenMP, all host threads) on a bounded number of steps of the same workload."""
+    t0 = time.perf_counter()
+    case = make_oracle(O, wl)
+    build_s = time.perf_counter() - t0
+    cells = int(case.fluid().sum())
+    threads = O.max_threads()
+    t0 = time.perf_counter()
+    steps = 0
+    while True:
+        case.run(1, CFL)
+        steps += 1
+        el = time.perf_counter() - t0
+        if el > budget_s or (el / steps) * (steps + 1) > budget_s * 1.5:
+            break
+    return {"value": cells * steps / el, "unit": "cell-updates/s", "cores": threads, "kind": "port",
+            "sample": f"{steps} SSP-RK3 step(s) of the {wl} workload ({cells} fluid cells), "
+                      f"{el:.1f} s, after a {build_s:.1f} s ghost-grid build"}
+
+
+def run_reference(args):
+    from oracle import oracle as O
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    spec = WORKLOADS[args.workload]
+    case = make_oracle(O, args.workload)
+    cells = int(case.fluid().sum())
+    threads = O.max_threads()
+    for _ in range(min(args.warmup, 1)):
+        case.run(1, CFL)
+    # each timed step is one full SSP-RK3 step; the number of steps is capped so
+    # the run stays within a few minutes
+    t0 = time.perf_counter()
+    steps = 0
+    while steps < args.steps:
+        case.run(1, CFL)
+        steps += 1
+        if time.perf_counter() - t0 > 120.0:
+            break
+    el = time.perf_counter() - t0
+    v = cells * steps / el
+    line = {"metric": "cell-updates/s", "value": v, "unit": "cell-updates/s", "n_gpus": args.gpus,
+            "steps": steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": spec["name"], "fluid_cells": cells},
+            "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": threads, "kind": "port",
+                             "sample": f"{steps} of {args.steps} requested SSP-RK3 steps (capped at ~120 s)"},
+            "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="cyl961", choices=sorted(WORKLOADS))
+    ap.add_argument("--exact", action="store_true", help="bench the no-FMA-contraction build")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import importlib
+    import torch
+
+    rh = importlib.import_module("3t_rh_b200")
+    from importlib import import_module
+    flops = import_module("3t_rh_b200.flops")
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device(f"cuda:{local}"))
+
+    spec = WORKLOADS[args.workload]
+    f = make_field(rh, args.workload)
+    t0 = time.perf_counter()
+    g = rh.GhostGrid.build(f)
+    build_s = time.perf_counter() - t0
+    s = rh.Solver(f, g, device=local, exact=args.exact)
+    cells = int(f.fluid.sum())
+    nxf, nyf = flops.face_counts(f.fluid, f.grid.nx, f.grid.ny)
+    diff = bool(any(getattr(f.params, k) != 0.0 for k in ("kappa_e", "kappa_i", "kappa_r")))
+    src = bool(any(getattr(f.params, k) != 0.0 for k in ("omega_ei", "omega_er")))
+    step_fl = flops.step_flops(cells, nxf, nyf, g.len(), g.n_heavy(), diff, src)
+    stream = torch.cuda.ExternalStream(s.stream, device=torch.device(f"cuda:{local}"))
+
+    s.advance(args.warmup, CFL)
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = s.kernel_launches
+    ev0.record(stream)
+    s.advance(args.steps, CFL)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    launches = s.kernel_launches - l0
+    if dist:
+        t = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    sampler.stop()
+    clocks = sampler.summary()
+    value = world * cells * args.steps / (ms * 1e-3)
+
+    # roofline of the dominant kernel: live per-launch durations (CUDA events)
+    prof = s.profile_steps(min(args.steps, 20), CFL)
+    flux_ms, flux_n = prof["flux"]
+    fl_launch = flops.flux_launch_flops(nxf, nyf, diff)
+    achieved = fl_launch / (flux_ms / flux_n * 1e-3) / 1e12
+    peak = rh.api.fp64_peak_tflops(local)
+    total_prof_ms = sum(v[0] for v in prof.values())
+
+    e2e = None
+    if not args.no_e2e:
+        n = f.grid.len()
+        host = torch.empty((n, 6), dtype=torch.float64, pin_memory=True).numpy()
+        u, tcur = s.download()
+        host[:] = u
+        k_e2e = max(3, min(args.steps, 20))
+        s.step_host(host, tcur, CFL)  # warm
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(k_e2e):
+            tcur, _dt = s.step_host(host, tcur, CFL)
+        el = time.perf_counter() - t0
+        e2e = {"value": world * cells * k_e2e / el, "unit": "cell-updates/s",
+               "h2d_bytes_per_step": n * 6 * 8, "d2h_bytes_per_step": n * 6 * 8 + 16,
+               "call": "rh3t_step_host (upload Field::value, dt reduction, rk3_ssp, download)", "steps": k_e2e}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        from oracle import oracle as O  # timed CPU baseline only
+        cpu = cpu_baseline(O, args.workload)
+
+    if rank == 0:
+        line = {
+            "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": spec["name"], "scheme": "SSP-RK3, dt = 0.05 dt_cfl per step", "grid":
+                       [f.grid.nx, f.grid.ny], "fluid_cells": cells, "ghosts": g.len(), "heavy_ghosts": g.n_heavy(),
+                       "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "inputs larger than L2 (state buffers 3 x %.0f MB)" % (
+                           6 * 8 * (f.grid.nx + 8) * (f.grid.ny + 8) / 1e6),
+                       "arithmetic": "no FMA contraction" if args.exact else "FMA contraction",
+                       "ghost_build_s": round(build_s, 3)},
+            "roofline": {"bound": "fp64", "kernel": "k_flux (x+y interface WENO5 fluxes)", "achieved": achieved,
+                         "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                         "peak_source": "measured DFMA loop on this GPU (rh3t_fp64_peak)",
+                         "flops_per_launch": fl_launch, "launch_ms": flux_ms / flux_n,
+                         "kernel_share": {k: v[0] / total_prof_ms for k, v in prof.items()},
+                         "step_tflops": step_fl / (ms / args.steps * 1e-3) / 1e12,
+                         "step_flops": step_fl},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    s.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

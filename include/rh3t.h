@@ -197,6 +197,17 @@ int rh3t_step_host(rh3t_ctx* ctx, double* value, double* time, double cfl_factor
 /* dt of the last step of rh3t_advance / rh3t_step_host (host read) */
 int rh3t_last_dt(rh3t_ctx* ctx, double* dt);
 
+/* Instrumentation (no reference counterpart): runs nsteps steps of
+ * rh3t_advance without graph capture, with CUDA events around every launch,
+ * and returns the summed device time per kernel class in ms_out[0..4]:
+ * ghost update, interface fluxes, RHS + stage update, dt reduction, and the
+ * number of launches of each class in launches_out[0..4] (may be NULL). */
+int rh3t_profile_steps(rh3t_ctx* ctx, int32_t nsteps, double cfl_factor, double* ms_out, int64_t* launches_out);
+
+/* Measured FP64 FMA throughput of the device (TFLOP/s, 2 FLOP per FMA) from a
+ * register-resident DFMA loop over all SMs; the FP64 roofline denominator. */
+int rh3t_fp64_peak(int32_t device, double* tflops);
+
 int rh3t_synchronize(rh3t_ctx* ctx);
 int rh3t_last_error(const rh3t_ctx* ctx, rh3t_error* out);
 /* number of kernels this context launched since creation (instrumentation) */

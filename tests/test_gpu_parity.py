@@ -1,0 +1,136 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle.
+
+Tolerance (normwise relative L-infinity per field over fluid nodes,
+max|gpu - oracle| / max|oracle|):
+  - librh3t_exact (no FMA contraction): l() <= 1e-13, 100 RK3 steps <= 1e-12
+    (the only arithmetic that differs from the oracle is CUDA's pow() in the
+    boundary WENO weights and in Tr);
+  - librh3t (FMA contraction): l() <= 1e-11, N steps <= 1e-10 (the target).
+"""
+import math
+
+import numpy as np
+import pytest
+
+from helpers import rel_linf
+
+pytestmark = pytest.mark.gpu
+
+
+def _pair(rh, O, case="cylinder", **kw):
+    if case == "cylinder":
+        f = rh.cases.init_cylinder(**kw)
+        ref = O.Case.cylinder(**kw)
+    elif case == "planar":
+        p = dict(kappa_e=1e-3, kappa_i=1e-3, kappa_r=1e-3, omega_ei=1.0, omega_er=1.0, periodic_ly=0.03125)
+        f = rh.cases.planar_shock(params=rh.Params(**p), **kw)
+        ref = O.Case.planar_shock(**kw, **p)
+    elif case == "dmr":
+        f = rh.cases.init_double_mach(**kw)
+        ref = O.Case.double_mach(**kw)
+    else:
+        raise ValueError(case)
+    assert np.array_equal(f.value, ref.state())
+    return f, rh.GhostGrid.build(f), ref
+
+
+@pytest.mark.parametrize("exact,tol", [(True, 1e-13), (False, 1e-11)])
+def test_l_cylinder(rh, O, exact, tol):
+    f, g, ref = _pair(rh, O)
+    ref.run(20)  # a developed bow-shock state, the same input for both
+    f.value[:] = ref.state()
+    f.time = ref.time
+    s = rh.Solver(f, g, exact=exact)
+    rhs, gv = s.l(with_ghosts=True)
+    rr, rg = ref.l()
+    e_rhs = rel_linf(rhs, rr, f.fluid).max()
+    e_g = rel_linf(gv, rg, np.ones(len(rg), bool)).max()
+    print(f"l() exact={exact}: rhs {e_rhs:.3e}, ghosts {e_g:.3e}")
+    assert e_rhs <= tol and e_g <= tol
+
+
+def test_global_dt_bit_exact(rh, O):
+    f, g, ref = _pair(rh, O)
+    ref.run(10)
+    f.value[:] = ref.state()
+    s = rh.Solver(f, g, exact=True)
+    assert s.calc_global_dt() == ref.global_dt()
+    s2 = rh.Solver(f, g, exact=False)
+    assert abs(s2.calc_global_dt() - ref.global_dt()) <= 1e-15 * ref.global_dt()
+
+
+@pytest.mark.parametrize("exact,tol", [(True, 1e-12), (False, 1e-10)])
+def test_rk3_cylinder_100_steps(rh, O, exact, tol):
+    f, g, ref = _pair(rh, O)
+    s = rh.Solver(f, g, exact=exact)
+    s.advance(100, 0.05)
+    dts = ref.run(100, 0.05)
+    u, t = s.download()
+    err = rel_linf(u, ref.state(), f.fluid)
+    print(f"cylinder 121x481 100 steps exact={exact}: per-field {err}")
+    assert err.max() <= tol
+    assert abs(t - ref.time) <= 1e-12 * ref.time
+    assert abs(s.last_dt() - dts[-1]) <= 1e-10 * dts[-1]
+
+
+@pytest.mark.parametrize("exact,tol", [(True, 1e-12), (False, 1e-10)])
+def test_planar_shock_periodic_outflow_diffusion_source(rh, O, exact, tol):
+    f, g, ref = _pair(rh, O, "planar")
+    s = rh.Solver(f, g, exact=exact)
+    s.advance(100, 0.05)
+    ref.run(100, 0.05)
+    u, _ = s.download()
+    err = rel_linf(u, ref.state(), f.fluid)
+    print(f"planar shock 1024x8 100 steps exact={exact}: per-field {err}")
+    assert err.max() <= tol
+
+
+def test_graph_and_eager_identical(rh, O):
+    f, g, _ = _pair(rh, O)
+    a = rh.Solver(f, g)
+    b = rh.Solver(f, g)
+    a.advance(10, 0.05, graph=True)
+    b.advance(10, 0.05, graph=False)
+    ua, ta = a.download()
+    ub, tb = b.download()
+    assert np.array_equal(ua, ub) and ta == tb
+
+
+def test_deterministic_runs(rh, O):
+    f, g, _ = _pair(rh, O)
+    outs = []
+    for _ in range(2):
+        s = rh.Solver(f, g)
+        s.advance(20, 0.05)
+        outs.append(s.download()[0])
+    assert np.array_equal(outs[0], outs[1])
+
+
+def test_rk3_ssp_given_dt_and_host_step(rh, O):
+    f, g, ref = _pair(rh, O)
+    s = rh.Solver(f, g, exact=True)
+    dt = 0.05 * ref.global_dt()
+    s.rk3_ssp(dt)
+    ref.rk3_ssp(dt)
+    u, t = s.download()
+    assert rel_linf(u, ref.state(), f.fluid).max() <= 1e-13
+    # drop-in loop body with a host value array (main.rs:460-466)
+    v = np.ascontiguousarray(f.value.copy())
+    s2 = rh.Solver(f, g, exact=True)
+    t2, dt2 = s2.step_host(v, 0.0, 0.05)
+    ref2 = O.Case.cylinder()
+    ref2.run(1, 0.05)
+    assert rel_linf(v, ref2.state(), f.fluid).max() <= 1e-13
+    assert t2 == ref2.time
+
+
+def test_nonphysical_state_reported(rh, O):
+    f, g, _ = _pair(rh, O, h=1.0 / 10.0)
+    bad = f.value.copy()
+    k = np.flatnonzero(f.fluid)[100]
+    bad[k, 0] = -1.0  # negative density in one cell, injected on the host
+    f.value[:] = bad
+    s = rh.Solver(f, g)
+    with pytest.raises(rh.RH3TError) as ei:
+        s.advance(3, 0.05)
+    assert ei.value.kind in ("NONPHYSICAL_STATE", "NONFINITE_GHOST", "NONPOSITIVE_DT")
