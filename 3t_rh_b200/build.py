@@ -23,9 +23,9 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 GXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CU_SOURCES = ["kernels.cu", "context.cu"]
+CU_SOURCES = ["kernels.cu", "flux.cu", "context.cu"]
 CPP_SOURCES = ["host/ghostgrid.cpp"]
-HEADERS = ["physics.cuh", "rh3t_dev.h", "kernels.cuh"]
+HEADERS = ["physics.cuh", "rh3t_dev.h", "kernels.cuh", "common.cuh"]
 
 
 def _run(cmd):
@@ -60,7 +60,8 @@ def build(force=False, verbose=False):
         objs = []
         for src in CU_SOURCES:
             obj = os.path.join(OUT, f"{os.path.splitext(src)[0]}_{fmad}.o")
-            log = _run([NVCC] + ARCH + ["-O3", "-lineinfo", "-std=c++17", f"--fmad={fmad}", "-Xptxas", "-v",
+            defs = ["-DRH3T_EXACT"] if fmad == "false" else []
+            log = _run([NVCC] + ARCH + defs + ["-O3", "-lineinfo", "-std=c++17", f"--fmad={fmad}", "-Xptxas", "-v",
                                         "-Xcompiler", "-fPIC,-ffp-contract=off", "-I", INCLUDE, "-c",
                                         os.path.join(CSRC, src), "-o", obj])
             if verbose:

@@ -220,16 +220,19 @@ extern "C" int rh3t_create(const rh3t_grid* grid, const rh3t_params* params, con
     // ---- tiles
     std::vector<Tile> tx, ty, tc;
     auto isf = [&](long i, long j) { return i >= 0 && i < nx && j >= 0 && j < ny && fluid[(size_t)i * ny + j]; };
-    for (long i = 0; i <= nx; ++i)
-        for (long j0 = 0; j0 < ny; j0 += TILE) {
+    // x faces (i - 1/2, j), i in [0, nx]: tiles of FX_TI x FX_TJ faces
+    for (long i0 = 0; i0 <= nx; i0 += FX_TI)
+        for (long j0 = 0; j0 < ny; j0 += FX_TJ) {
             bool any = false;
-            for (long j = j0; j < std::min(ny, j0 + TILE) && !any; ++j) any = isf(i, j) || isf(i - 1, j);
-            if (any) tx.push_back({0, (int)i, (int)j0, 0});
+            for (long i = i0; i < std::min(nx + 1, i0 + FX_TI) && !any; ++i)
+                for (long j = j0; j < std::min(ny, j0 + FX_TJ) && !any; ++j) any = isf(i, j) || isf(i - 1, j);
+            if (any) tx.push_back({0, (int)i0, (int)j0, 0});
         }
+    // y faces (i, j - 1/2), j in [0, ny]: tiles of FY_TJ faces along j
     for (long i = 0; i < nx; ++i)
-        for (long j0 = 0; j0 <= ny; j0 += TILE) {
+        for (long j0 = 0; j0 <= ny; j0 += FY_TJ) {
             bool any = false;
-            for (long j = j0; j <= std::min(ny, j0 + TILE - 1) && !any; ++j) any = isf(i, j) || isf(i, j - 1);
+            for (long j = j0; j <= std::min(ny, j0 + FY_TJ - 1) && !any; ++j) any = isf(i, j) || isf(i, j - 1);
             if (any) ty.push_back({0, (int)i, (int)j0, 0});
         }
     for (long i = 0; i < nx; ++i)
@@ -595,6 +598,26 @@ extern "C" int rh3t_fp64_peak(int32_t device, double* tflops) {
     if (e != cudaSuccess) return RH3T_ERR_CUDA;
     *tflops = best;
     return RH3T_OK;
+}
+
+extern "C" int rh3t_math_check(int32_t device, const double* x, int32_t n, double q, double* out) {
+    if (!x || !out || n < 0) return RH3T_ERR_INVALID_ARGUMENT;
+    if (cudaSetDevice(device) != cudaSuccess) return RH3T_ERR_NO_DEVICE;
+    double *dx = nullptr, *dout = nullptr;
+    if (cudaMalloc(&dx, (size_t)std::max(n, 1) * sizeof(double)) != cudaSuccess) return RH3T_ERR_CUDA;
+    if (cudaMalloc(&dout, (size_t)std::max(n, 1) * 3 * sizeof(double)) != cudaSuccess) {
+        cudaFree(dx);
+        return RH3T_ERR_CUDA;
+    }
+    cudaError_t e = cudaMemcpy(dx, x, (size_t)n * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && n > 0) {
+        launch_math_check(0, dx, n, q, dout);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(out, dout, (size_t)n * 3 * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(dx);
+    cudaFree(dout);
+    return e == cudaSuccess ? RH3T_OK : RH3T_ERR_CUDA;
 }
 
 extern "C" int rh3t_last_dt(rh3t_ctx* c, double* dt) {

@@ -6,32 +6,11 @@
 // Per RK stage: k_ghosts (ghost.rs:199-268) -> k_flux (main.rs:165-246) ->
 // k_rhs_stage (main.rs:251-349). Per step: k_dt (main.rs:375-408, dt.rs)
 // first. dt, stage times and RK coefficients never leave the device.
+#include "common.cuh"
 #include "kernels.cuh"
 #include "physics.cuh"
 
 namespace rh3t {
-
-__device__ __forceinline__ long long node_of(const Inst& I, int i, int j) {
-    return (long long)(i + RH3T_PAD) * I.nyp + (j + RH3T_PAD);
-}
-
-__device__ __forceinline__ void load6(const double* __restrict__ buf, long long plane, long long n, double s[6]) {
-#pragma unroll
-    for (int c = 0; c < 6; ++c) s[c] = buf[c * plane + n];
-}
-
-__device__ __forceinline__ bool has_error(const Inst& I) { return I.err->key != ~0ull; }
-
-__device__ __forceinline__ void report(const Inst& I, int phase, int code, unsigned int index) {
-    unsigned long long step = (unsigned long long)I.sc->step;
-    unsigned long long key = (step << 40) | ((unsigned long long)phase << 37) | ((unsigned long long)code << 32) |
-                             (unsigned long long)index;
-    atomicMin(&I.err->key, key);
-}
-
-__device__ __forceinline__ const double* stage_src(const Inst& I, int stage) {
-    return stage == 0 ? I.U : (stage == 1 ? I.A : I.B);
-}
 
 // ------------------------------------------------------------------ ghosts
 // 6 threads per ghost (threadIdx.x = characteristic component c), 32 ghosts
@@ -207,7 +186,7 @@ __global__ void __launch_bounds__(192) k_ghosts(const Inst* __restrict__ insts, 
         double alpha[5], asum = 0.0;
 #pragma unroll
         for (int r = 0; r < 5; ++r) {
-            alpha[r] = hv_d[h * 5 + r] / pow(P.eps + beta[r], P.weno_q);
+            alpha[r] = hv_d[h * 5 + r] / pow_q(P.eps + beta[r], P.weno_q);
             asum += alpha[r];
         }
 #pragma unroll
@@ -301,100 +280,6 @@ __global__ void __launch_bounds__(192) k_ghosts(const Inst* __restrict__ insts, 
         wbuf[k * plane + R.node] = out[k];
     }
     if (!fin) report(I, 1 + 2 * stage, 2, (unsigned)R.gid);
-}
-
-// ------------------------------------------------------------------ fluxes
-// One thread per interface. The characteristic loop is outermost: for each
-// characteristic field c the thread forms row c of L, the six projected
-// fluxes/states, the two WENO5 reconstructions and accumulates column c of
-// R, which keeps the reference's association of R.(f+ + f-) (weno.rs:685-802).
-template <int DIR>
-__device__ __forceinline__ void face_flux(const Inst& I, const double* __restrict__ buf, int i, int j,
-                                          double* __restrict__ fout, long long fplane, long long fidx,
-                                          double* __restrict__ dout) {
-    const DevParams& P = I.P;
-    const long long plane = I.plane;
-    double s[6][6], F[6][6];
-    Prim d2, d3;
-#pragma unroll
-    for (int p = 0; p < 6; ++p) {
-        long long n = DIR == 0 ? node_of(I, i - 3 + p, j) : node_of(I, i, j - 3 + p);
-        load6(buf, plane, n, s[p]);
-        Prim d = prim_from_state(s[p], P);
-        phys_flux<DIR>(s[p], d, F[p]);
-        if (p == 2) d2 = d;
-        if (p == 3) d3 = d;
-    }
-    Roe q = roe_average(s[3][0], d3, s[2][0], d2, P);
-    double out[6];
-#pragma unroll
-    for (int c = 0; c < 6; ++c) {
-        double Lc[6], Rc[6], lam;
-        l_row<DIR>(c, q, P, Lc);
-        r_col<DIR>(c, q, P, Rc, lam);
-        double a = fabs(lam);
-        double fp[6], fm[6];
-#pragma unroll
-        for (int p = 0; p < 6; ++p) {
-            double cf = Lc[0] * F[p][0] + Lc[1] * F[p][1] + Lc[2] * F[p][2] + Lc[3] * F[p][3] + Lc[4] * F[p][4] +
-                        Lc[5] * F[p][5];
-            double cs = Lc[0] * s[p][0] + Lc[1] * s[p][1] + Lc[2] * s[p][2] + Lc[3] * s[p][3] + Lc[4] * s[p][4] +
-                        Lc[5] * s[p][5];
-            fp[p] = 0.5 * (cf + a * cs);
-            fm[p] = 0.5 * (cf - a * cs);
-        }
-        double g = weno5(fp[0], fp[1], fp[2], fp[3], fp[4], P.eps) + weno5(fm[5], fm[4], fm[3], fm[2], fm[1], P.eps);
-#pragma unroll
-        for (int k = 0; k < 6; ++k) out[k] = c == 0 ? Rc[k] * g : out[k] + Rc[k] * g;
-    }
-#pragma unroll
-    for (int k = 0; k < 6; ++k) fout[k * fplane + fidx] = out[k];
-    if (dout) {
-        // diffusion.rs:27-50 on the same six points
-        double te[6], ti[6], tr[6];
-#pragma unroll
-        for (int p = 0; p < 6; ++p) temps_from_state(s[p], P, te[p], ti[p], tr[p]);
-        double ee_t = P.kappa_e * (2.0 * te[5] - 25.0 * te[4] + 245.0 * te[3] - 245.0 * te[2] + 25.0 * te[1] - 2.0 * te[0]);
-        double ei_t = P.kappa_i * (2.0 * ti[5] - 25.0 * ti[4] + 245.0 * ti[3] - 245.0 * ti[2] + 25.0 * ti[1] - 2.0 * ti[0]);
-        double er_t = P.kappa_r * (2.0 * pow4d(tr[5]) - 25.0 * pow4d(tr[4]) + 245.0 * pow4d(tr[3]) -
-                                   245.0 * pow4d(tr[2]) + 25.0 * pow4d(tr[1]) - 2.0 * pow4d(tr[0]));
-        dout[fidx] = ee_t / 180.0;
-        dout[fplane + fidx] = ei_t / 180.0;
-        dout[2 * fplane + fidx] = er_t / 180.0;
-    }
-}
-
-__global__ void __launch_bounds__(128) k_flux(const Inst* __restrict__ insts, const Tile* __restrict__ tx, int ntx,
-                                              const Tile* __restrict__ ty, int nty, int stage) {
-    const int b = blockIdx.x;
-    if (b < ntx) {
-        const Tile t = tx[b];
-        const Inst& I = insts[t.inst];
-        const int j = t.j0 + threadIdx.x;
-        if (j >= I.ny || has_error(I)) return;
-        const int i = t.i;
-        if (!(I.mask[node_of(I, i, j)] | I.mask[node_of(I, i - 1, j)])) {
-            const long long fp = (long long)(I.nx + 1) * I.ny, fi = (long long)i * I.ny + j;
-#pragma unroll
-            for (int k = 0; k < 6; ++k) I.fx[k * fp + fi] = 0.0;
-            return;
-        }
-        const long long fp = (long long)(I.nx + 1) * I.ny;
-        face_flux<0>(I, stage_src(I, stage), i, j, I.fx, fp, (long long)i * I.ny + j, I.diffusion ? I.dfx : nullptr);
-    } else if (b < ntx + nty) {
-        const Tile t = ty[b - ntx];
-        const Inst& I = insts[t.inst];
-        const int j = t.j0 + threadIdx.x;
-        if (j > I.ny || has_error(I)) return;
-        const int i = t.i;
-        const long long fp = (long long)I.nx * (I.ny + 1), fi = (long long)i * (I.ny + 1) + j;
-        if (!(I.mask[node_of(I, i, j)] | I.mask[node_of(I, i, j - 1)])) {
-#pragma unroll
-            for (int k = 0; k < 6; ++k) I.fy[k * fp + fi] = 0.0;
-            return;
-        }
-        face_flux<1>(I, stage_src(I, stage), i, j, I.fy, fp, fi, I.diffusion ? I.dfy : nullptr);
-    }
 }
 
 // ------------------------------------------------------------------ rhs + stage
@@ -658,7 +543,21 @@ __global__ void __launch_bounds__(256) k_dfma(double* out, int iters, double b, 
     if (s == 12345.678) out[blockIdx.x] = s; // never true; keeps the loop live
 }
 
+// ------------------------------------------------------------------ math check
+// out[3k] = x^(1/4), out[3k+1] = x^10, out[3k+2] = x^q with the device
+// routines used by the solver (diagnostic entry rh3t_math_check).
+__global__ void k_math_check(const double* __restrict__ x, int n, double q, double* __restrict__ out) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    out[3 * k] = cr_pow_quarter(x[k]);
+    out[3 * k + 1] = cr_powi(x[k], 10);
+    out[3 * k + 2] = pow_q(x[k], q);
+}
+
 // ------------------------------------------------------------------ host launchers
+void launch_math_check(cudaStream_t s, const double* x, int n, double q, double* out) {
+    k_math_check<<<(n + 127) / 128, 128, 0, s>>>(x, n, q, out);
+}
 void launch_dfma(cudaStream_t s, int blocks, double* out, int iters) {
     k_dfma<<<blocks, 256, 0, s>>>(out, iters, 0.9999999, 1e-7);
 }
@@ -668,10 +567,6 @@ void launch_ghosts(cudaStream_t s, const Inst* insts, const GhostRec* recs, int 
     if (n <= 0) return;
     dim3 blk(6, 32);
     k_ghosts<<<(n + 31) / 32, blk, 0, s>>>(insts, recs, n, hst, hs, hw, hd, stage);
-}
-void launch_flux(cudaStream_t s, const Inst* insts, const Tile* tx, int ntx, const Tile* ty, int nty, int stage) {
-    if (ntx + nty <= 0) return;
-    k_flux<<<ntx + nty, 128, 0, s>>>(insts, tx, ntx, ty, nty, stage);
 }
 void launch_rhs_stage(cudaStream_t s, const Inst* insts, const Tile* tc, int nt, int stage, int mode, double* rhs) {
     if (nt <= 0) return;

@@ -15,4 +15,5 @@ void launch_gather(cudaStream_t s, const Inst* insts, int inst, long long ncell,
 void launch_planes_to_aos(cudaStream_t s, const double* planes, long long n, double* aos);
 void launch_ghost_values(cudaStream_t s, const Inst* insts, const GhostRec* recs, int n, double* out);
 void launch_dfma(cudaStream_t s, int blocks, double* out, int iters);
+void launch_math_check(cudaStream_t s, const double* x, int n, double q, double* out);
 } // namespace rh3t

@@ -12,6 +12,65 @@ namespace rh3t {
 __device__ __forceinline__ double sqd(double x) { return x * x; }
 __device__ __forceinline__ double pow4d(double x) { return (x * x) * (x * x); }
 
+// ---- correctly rounded powers for the two pow() calls of the reference
+// (state.rs:261 powf(0.25), bc1.rs:241 powf(WENO_Q)). Double-double
+// arithmetic (Dekker 1971: exact product by FMA, normalised sums) carries
+// ~104 significant bits, so rounding the double-double result gives the
+// correctly rounded power except within ~1e-31 of a rounding midpoint.
+// Explicit __fma_rn / __dmul_rn / __dadd_rn keep the sequence identical in
+// the FMA and the no-contraction builds.
+struct DD {
+    double hi, lo;
+};
+__device__ __forceinline__ DD dd_sq(double a) {
+    double p = __dmul_rn(a, a);
+    return {p, __fma_rn(a, a, -p)};
+}
+__device__ __forceinline__ DD dd_mul(DD a, DD b) {
+    double p = __dmul_rn(a.hi, b.hi);
+    double e = __fma_rn(a.hi, b.hi, -p);
+    e = __fma_rn(a.hi, b.lo, e);
+    e = __fma_rn(a.lo, b.hi, e);
+    double s = __dadd_rn(p, e);
+    return {s, __dsub_rn(e, __dsub_rn(s, p))};
+}
+// x^n for an integer n >= 1 by binary powering in double-double
+__device__ __forceinline__ double cr_powi(double x, int n) {
+    if (!isfinite(x) || x == 0.0) return pow(x, (double)n);
+    DD r = {1.0, 0.0}, a = {x, 0.0};
+    bool first = true;
+    while (n > 0) {
+        if (n & 1) { r = first ? a : dd_mul(r, a); first = false; }
+        n >>= 1;
+        if (n) a = (a.lo == 0.0) ? dd_sq(a.hi) : dd_mul(a, a);
+    }
+    if (!isfinite(r.hi)) return r.hi;
+    return __dadd_rn(r.hi, r.lo);
+}
+// x^(1/4): sqrt(sqrt(x)) is within one ulp; of it and its two neighbours pick
+// the one whose fourth power (double-double) is nearest to x.
+__device__ __forceinline__ double cr_pow_quarter(double x) {
+    double y = sqrt(sqrt(x));
+    if (!(x > 0.0) || !isfinite(y) || !isfinite(x)) return y;
+    const long long yb = __double_as_longlong(y); // y > 0 and finite here: neighbours by bit pattern
+    double cand[3] = {__longlong_as_double(yb - 1), y, __longlong_as_double(yb + 1)};
+    double best = y, bd = INFINITY;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        DD c2 = dd_sq(cand[k]);
+        DD c4 = dd_mul(c2, c2);
+        double d = fabs(__dadd_rn(__dsub_rn(c4.hi, x), c4.lo));
+        if (d < bd || (d == bd && k == 1)) { bd = d; best = cand[k]; }
+    }
+    return best;
+}
+// powf(q) of the boundary WENO weights: integer q in double-double, else libdevice pow
+__device__ __forceinline__ double pow_q(double x, double q) {
+    if (q == 10.0) return cr_powi(x, 10);
+    if (q >= 1.0 && q <= 64.0 && q == floor(q)) return cr_powi(x, (int)q);
+    return pow(x, q);
+}
+
 // Subset of state.rs:245-276 Derived::from_state needed by fluxes, L/R and noncon.
 struct Prim {
     double u, v, e_e, e_i, e_r, pe, pi, pr;
@@ -39,7 +98,7 @@ __device__ __forceinline__ void temps_from_state(const double s[6], const DevPar
     te = s[3] / (s[0] * P.cve) - w2 / (6.0 * P.cve);
     ti = s[4] / (s[0] * P.cvi) - w2 / (6.0 * P.cvi);
     double er_term = s[5] / s[0] - w2 / 6.0;
-    tr = pow(er_term * s[0] / P.a_rad, 0.25);
+    tr = cr_pow_quarter(er_term * s[0] / P.a_rad);
 }
 
 // state.rs:56-85 flux_from_derived
@@ -197,6 +256,173 @@ __device__ __forceinline__ void r_col(int col, const Roe& q, const DevParams& P,
         }
     }
 }
+
+// Row `row` of the right eigenvector matrix (weno.rs:518-545) and the
+// eigenvalue of characteristic field `row`.
+template <int DIR>
+__device__ __forceinline__ void r_row(int row, const Roe& q, const DevParams& P, double R[6], double& lam) {
+    const double GE = P.gamma_e, GI = P.gamma_i, GR = P.gamma_r;
+    const double gi = GI - 1.0, ge = GE - 1.0, gr = GR - 1.0;
+    const double gt = gi + ge + gr;
+    const double u = q.u, v = q.v, w2 = q.w2, cs = q.cs;
+    const double vel = DIR == 0 ? u : v;
+    lam = row == 0 ? vel - cs : (row == 5 ? vel + cs : vel);
+    if (DIR == 0) {
+        switch (row) {
+        case 0: R[0] = 1.0; R[1] = 1.0; R[2] = 1.0; R[3] = 1.0; R[4] = 0.0; R[5] = 1.0; break;
+        case 1: R[0] = u - cs; R[1] = u; R[2] = u; R[3] = u; R[4] = 0.0; R[5] = u + cs; break;
+        case 2: R[0] = v; R[1] = v; R[2] = v; R[3] = v; R[4] = 1.0; R[5] = v; break;
+        case 3:
+            R[0] = GE * q.ee + w2 / 6.0 - u * cs / 3.0; R[1] = gt * w2 / (6.0 * ge); R[2] = -gr; R[3] = gi;
+            R[4] = v / 3.0; R[5] = GE * q.ee + w2 / 6.0 + u * cs / 3.0; break;
+        case 4:
+            R[0] = GI * q.ei + w2 / 6.0 - u * cs / 3.0; R[1] = gr; R[2] = gt * w2 / (6.0 * gi); R[3] = -ge;
+            R[4] = v / 3.0; R[5] = GI * q.ei + w2 / 6.0 + u * cs / 3.0; break;
+        default:
+            R[0] = GR * q.er + w2 / 6.0 - u * cs / 3.0; R[1] = -gi; R[2] = ge; R[3] = gt * w2 / (6.0 * gr);
+            R[4] = v / 3.0; R[5] = GR * q.er + w2 / 6.0 + u * cs / 3.0; break;
+        }
+    } else {
+        switch (row) {
+        case 0: R[0] = 1.0; R[1] = 0.0; R[2] = 1.0; R[3] = 1.0; R[4] = 1.0; R[5] = 1.0; break;
+        case 1: R[0] = u; R[1] = 1.0; R[2] = u; R[3] = u; R[4] = u; R[5] = u; break;
+        case 2: R[0] = v - cs; R[1] = 0.0; R[2] = v; R[3] = v; R[4] = v; R[5] = v + cs; break;
+        case 3:
+            R[0] = GE * q.ee + w2 / 6.0 - v * cs / 3.0; R[1] = u / 3.0; R[2] = gt * w2 / (6.0 * ge); R[3] = -gr;
+            R[4] = gi; R[5] = GE * q.ee + w2 / 6.0 + v * cs / 3.0; break;
+        case 4:
+            R[0] = GI * q.ei + w2 / 6.0 - v * cs / 3.0; R[1] = u / 3.0; R[2] = gr; R[3] = gt * w2 / (6.0 * gi);
+            R[4] = -ge; R[5] = GI * q.ei + w2 / 6.0 + v * cs / 3.0; break;
+        default:
+            R[0] = GR * q.er + w2 / 6.0 - v * cs / 3.0; R[1] = u / 3.0; R[2] = -gi; R[3] = ge;
+            R[4] = gt * w2 / (6.0 * gr); R[5] = GR * q.er + w2 / 6.0 + v * cs / 3.0; break;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- fast forms
+// Same mathematics, fewer divisions (shared reciprocals, a single division per
+// WENO5 reconstruction); used by the FMA build only. Rounding differs from the
+// reference by a few ulps per operation, like FMA contraction does.
+namespace fastm {
+
+__device__ __forceinline__ Prim prim(const double s[6], const DevParams& P) {
+    Prim d;
+    const double ir = 1.0 / s[0];
+    d.u = s[1] * ir;
+    d.v = s[2] * ir;
+    const double w2 = d.u * d.u + d.v * d.v;
+    const double k = w2 * (1.0 / 6.0);
+    d.e_e = s[3] * ir - k;
+    d.e_i = s[4] * ir - k;
+    d.e_r = s[5] * ir - k;
+    const double rk = s[0] * k;
+    d.pe = (P.gamma_e - 1.0) * (s[3] - rk);
+    d.pi = (P.gamma_i - 1.0) * (s[4] - rk);
+    d.pr = (P.gamma_r - 1.0) * (s[5] - rk);
+    return d;
+}
+
+// Roe average from (sqrt(rho), u, v, e_e, e_i, e_r) of points[3] (a) and points[2] (b)
+__device__ __forceinline__ Roe roe(const double a[6], const double b[6], const DevParams& P) {
+    Roe q;
+    const double inv = 1.0 / (a[0] + b[0]);
+    q.u = (a[1] * a[0] + b[1] * b[0]) * inv;
+    q.v = (a[2] * a[0] + b[2] * b[0]) * inv;
+    q.w2 = q.u * q.u + q.v * q.v;
+    q.ee = (a[3] * a[0] + b[3] * b[0]) * inv;
+    q.ei = (a[4] * a[0] + b[4] * b[0]) * inv;
+    q.er = (a[5] * a[0] + b[5] * b[0]) * inv;
+    const double GE = P.gamma_e, GI = P.gamma_i, GR = P.gamma_r;
+    const double gi = GI - 1.0, ge = GE - 1.0, gr = GR - 1.0;
+    const double gt = gi + ge + gr;
+    q.cs2 = GE * ge * q.ee + GI * gi * q.ei + GR * gr * q.er;
+    q.cs = sqrt(q.cs2);
+    q.he = 6.0 * gi * gr * (GI * q.ei - GR * q.er) + GE * gt * q.ee * q.w2;
+    q.hi = 6.0 * ge * gr * (GR * q.er - GE * q.ee) + GI * gt * q.ei * q.w2;
+    q.hr = 6.0 * ge * gi * (GE * q.ee - GI * q.ei) + GR * gt * q.er * q.w2;
+    q.b = gt * (36.0 * ge * gi * gr + gt * q.w2 * q.w2) * q.cs2;
+    q.den = 12.0 * q.cs2;
+    return q;
+}
+
+template <int DIR>
+__device__ __forceinline__ void l_row(int row, const Roe& q, const DevParams& P, double L[6]) {
+    const double GE = P.gamma_e, GI = P.gamma_i, GR = P.gamma_r;
+    const double gi = GI - 1.0, ge = GE - 1.0, gr = GR - 1.0;
+    const double gt = gi + ge + gr;
+    const double u = q.u, v = q.v, w2 = q.w2, cs = q.cs, cs2 = q.cs2;
+    const double ics2 = 1.0 / cs2, ib = 1.0 / q.b;
+    const double iden = ics2 * (1.0 / 12.0);
+    int mode;
+    if (DIR == 0) {
+        const int m[6] = {0, 2, 3, 4, 1, 5};
+        mode = m[row];
+    } else {
+        mode = row;
+    }
+    if (mode == 0 || mode == 5) {
+        const double sg = mode == 0 ? 6.0 : -6.0;
+        const double vn = DIR == 0 ? u : v;
+        L[0] = (gt * w2 + sg * vn * cs) * iden;
+        if (DIR == 0) {
+            L[1] = (-2.0 * gt * u - sg * cs) * iden;
+            L[2] = (-2.0 * gt * v) * iden;
+        } else {
+            L[1] = (-2.0 * gt * u) * iden;
+            L[2] = (-2.0 * gt * v - sg * cs) * iden;
+        }
+        L[3] = 6.0 * ge * iden;
+        L[4] = 6.0 * gi * iden;
+        L[5] = 6.0 * gr * iden;
+    } else if (mode == 1) {
+        if (DIR == 0) { L[0] = -v; L[1] = 0.0; L[2] = 1.0; }
+        else { L[0] = -u; L[1] = 1.0; L[2] = 0.0; }
+        L[3] = 0.0; L[4] = 0.0; L[5] = 0.0;
+    } else {
+        // electron / ion / radiation: gk = (ge, gi, gr)[k], hk = (he, hi, hr)[k]
+        const double gk = mode == 2 ? ge : (mode == 3 ? gi : gr);
+        const double hk = mode == 2 ? q.he : (mode == 3 ? q.hi : q.hr);
+        const double t = (hk - cs2 * w2) * ib;
+        L[0] = gk / gt - gk * w2 * (ics2 * (1.0 / 6.0)) - gk * gt * w2 * t;
+        L[1] = gk * u * (ics2 * (1.0 / 3.0)) + 2.0 * gk * gt * u * t;
+        L[2] = gk * v * (ics2 * (1.0 / 3.0)) + 2.0 * gk * gt * v * t;
+        const double igc = ics2 / gt;
+        const double c6 = 6.0 * gk * ib;
+        if (mode == 2) {
+            L[3] = -ge * ge * igc - c6 * (ge * hk - gt * cs2 * w2);
+            L[4] = -ge * gi * igc - c6 * gi * (hk - 6.0 * gr * cs2);
+            L[5] = -ge * gr * igc - c6 * gr * (hk + 6.0 * gi * cs2);
+        } else if (mode == 3) {
+            L[3] = -gi * ge * igc - c6 * ge * (hk + 6.0 * gr * cs2);
+            L[4] = -gi * gi * igc - c6 * (gi * hk - gt * cs2 * w2);
+            L[5] = -gi * gr * igc - c6 * gr * (hk - 6.0 * ge * cs2);
+        } else {
+            L[3] = -gr * ge * igc - c6 * ge * (hk - 6.0 * gi * cs2);
+            L[4] = -gr * gi * igc - c6 * gi * (hk + 6.0 * ge * cs2);
+            L[5] = -gr * gr * igc - c6 * (gr * hk - gt * cs2 * w2);
+        }
+    }
+}
+
+// WENO5 with one division: alpha_k = d_k / s_k^2 scaled by s0^2 s1^2 s2^2
+__device__ __forceinline__ double weno5(double u0, double u1, double u2, double u3, double u4, double eps) {
+    const double c1312 = 13.0 / 12.0;
+    double t2 = u2 - 2.0 * u3 + u4, r2 = 3.0 * u2 - 4.0 * u3 + u4;
+    double t1 = u1 - 2.0 * u2 + u3, r1 = u1 - u3;
+    double t0 = u0 - 2.0 * u1 + u2, r0 = u0 - 4.0 * u1 + 3.0 * u2;
+    double s0 = eps + (c1312 * t0 * t0 + 0.25 * r0 * r0);
+    double s1 = eps + (c1312 * t1 * t1 + 0.25 * r1 * r1);
+    double s2 = eps + (c1312 * t2 * t2 + 0.25 * r2 * r2);
+    s0 *= s0; s1 *= s1; s2 *= s2;
+    double a0 = 0.1 * (s1 * s2), a1 = 0.6 * (s0 * s2), a2 = 0.3 * (s0 * s1);
+    double p0 = u0 * (1.0 / 3.0) - u1 * (7.0 / 6.0) + u2 * (11.0 / 6.0);
+    double p1 = -u1 * (1.0 / 6.0) + u2 * (5.0 / 6.0) + u3 * (1.0 / 3.0);
+    double p2 = u2 * (1.0 / 3.0) + u3 * (5.0 / 6.0) - u4 * (1.0 / 6.0);
+    return (a0 * p0 + a1 * p1 + a2 * p2) / (a0 + a1 + a2);
+}
+
+} // namespace fastm
 
 // weno.rs:847-886 weno5 (WENO-JS, p = 2)
 __device__ __forceinline__ double weno5(double u0, double u1, double u2, double u3, double u4, double eps) {

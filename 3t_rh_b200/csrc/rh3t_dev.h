@@ -99,9 +99,16 @@ struct Inst {
     DevError* err;
 };
 
-// work tile: 128 consecutive j at one i
+// work tile. Cell tiles: 128 consecutive j at one i. x-face tiles: faces
+// i in [i, i+FX_TI) x j in [j0, j0+FX_TJ). y-face tiles: faces j in
+// [j0, j0+FY_TJ) at column i.
 struct Tile {
     int32_t inst, i, j0, pad_;
 };
+
+constexpr int CELL_TILE = 128;
+constexpr int FX_TI = 5, FX_TJ = 8, FY_TJ = 40;
+constexpr int FLUX_FACES = 40;                   // faces per flux block
+constexpr int FLUX_NPT = (FX_TI + 5) * FX_TJ;    // staged points per flux block (>= FY_TJ + 5)
 
 } // namespace rh3t

@@ -208,6 +208,12 @@ int rh3t_profile_steps(rh3t_ctx* ctx, int32_t nsteps, double cfl_factor, double*
  * register-resident DFMA loop over all SMs; the FP64 roofline denominator. */
 int rh3t_fp64_peak(int32_t device, double* tflops);
 
+/* Diagnostic (no reference counterpart): the device power routines the solver
+ * uses in place of the reference's two powf calls (state.rs:261 x^0.25,
+ * bc1.rs:241 x^WENO_Q): out[3k] = x[k]^0.25, out[3k+1] = x[k]^10,
+ * out[3k+2] = x[k]^q. */
+int rh3t_math_check(int32_t device, const double* x, int32_t n, double q, double* out);
+
 int rh3t_synchronize(rh3t_ctx* ctx);
 int rh3t_last_error(const rh3t_ctx* ctx, rh3t_error* out);
 /* number of kernels this context launched since creation (instrumentation) */

@@ -84,6 +84,9 @@ def lib():
             ("oracle_circle_from_three", None, [dp, I, dp]),
             ("oracle_arc_project", None, [dp, I, D, D, dp]),
             ("oracle_arc_contains", I, [dp, I, D]),
+            ("oracle_ghost_extrapolation", I, [P, LG, dp]),
+            ("oracle_ghost_id", LG, [P, LG, LG]),
+            ("oracle_flop_counts", None, [C.c_void_p]),
         ]:
             f = getattr(L, name)
             f.restype = res
@@ -263,6 +266,15 @@ class Case:
             raise OracleError(rc, "ghost value", (gid, 0))
         return out
 
+    def ghost_id(self, i, j):
+        return int(lib().oracle_ghost_id(self.h, i, j))
+
+    def ghost_extrapolation(self, gid):
+        out = np.zeros((5, 6))
+        if lib().oracle_ghost_extrapolation(self.h, gid, _dp(out)):
+            raise ValueError("not a WENO-extrapolated ghost")
+        return out
+
     def extractor(self, proj5, r):
         out = np.zeros(((r + 1) ** 2, 2), np.int32)
         p = np.asarray(proj5, dtype=np.float64)
@@ -286,6 +298,13 @@ def max_threads():
 
 
 # ---- pointwise known-answer helpers
+def flop_counts():
+    out = np.zeros(11, np.int64)
+    lib().oracle_flop_counts(out.ctypes.data)
+    return dict(zip(("flux_x", "flux_y", "derived", "noncon_dir", "diffusion", "source", "local_dt", "weno5",
+                     "build_l", "build_r", "phys_flux"), out.tolist()))
+
+
 def weno5(u5):
     u = np.asarray(u5, dtype=np.float64)
     out = np.zeros(1)

@@ -967,6 +967,24 @@ int oracle_ghost_value(void* h, long id, double* out6) {
         return 0;
     } catch (OracleError& e) { return e.code; }
 }
+// V^(k) (k = 0..4, 6 characteristic components) of a heavy ghost: bc1.rs:193-255
+int oracle_ghost_extrapolation(void* h, long id, double* v30) {
+    Solver& s = ((Handle*)h)->s;
+    const GhostInfo& g = s.gg.info[id];
+    if (g.pre < 0) return -1;
+    const GhostBC& pre = s.gg.pre[g.pre];
+    double L[6][6], R[6][6], lam[6], v[5][6];
+    build_local_plain(g.project.normal, s.f.value[s.f.linear_index(pre.nearest_i, pre.nearest_j)], s.P, L, R, lam);
+    weno_extrapolation_all(L, pre, s.f.value.data(), s.P, v);
+    std::memcpy(v30, v, sizeof(v));
+    return 0;
+}
+long oracle_ghost_id(void* h, long i, long j) {
+    GhostGrid& gg = ((Handle*)h)->s.gg;
+    auto it = gg.lookup.find({i, j});
+    return it == gg.lookup.end() ? -1 : (long)it->second;
+}
+
 // arc description for the cylinder (three points used to build it)
 void oracle_arc(void* h, int which, double* out) {
     Field& f = ((Handle*)h)->s.f;

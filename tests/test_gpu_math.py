@@ -1,0 +1,28 @@
+"""Device power routines (x^(1/4) for Tr, x^10 for the boundary WENO weights)
+against correctly rounded values from mpmath. The reference calls libm pow
+(state.rs:261, bc1.rs:241); the device replaces both with correctly rounded
+double-double evaluations (3t_rh_b200/csrc/physics.cuh)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_correctly_rounded_powers(rh):
+    mpmath = pytest.importorskip("mpmath")
+    mpmath.mp.prec = 200
+    rng = np.random.default_rng(7)
+    x = np.concatenate([np.exp(rng.uniform(-20, 20, 3000)), np.exp(rng.uniform(-27.6, 5, 1000))])
+    L = rh.load()
+    out = np.zeros(3 * len(x))
+    assert L.rh3t_math_check(0, x.ctypes.data, len(x), 10.0, out.ctypes.data) == 0
+    out = out.reshape(-1, 3)
+    bad_q = bad_10 = 0
+    for k, v in enumerate(x):
+        m = mpmath.mpf(float(v))
+        bad_q += out[k, 0] != float(m ** mpmath.mpf(0.25))
+        bad_10 += out[k, 1] != float(m ** 10)
+    assert bad_q == 0 and bad_10 == 0, (bad_q, bad_10)
+    assert np.array_equal(out[:, 1], out[:, 2])
