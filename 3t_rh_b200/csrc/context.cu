@@ -19,7 +19,7 @@ using namespace rh3t;
 
 namespace {
 
-constexpr int TILE = 128;
+constexpr int TILE = CELL_TILE;
 
 template <class T> cudaError_t dalloc(T** p, size_t n) { return cudaMalloc((void**)p, n * sizeof(T) + 16); }
 
@@ -45,9 +45,10 @@ struct rh3t_ctx {
     Tile* d_tx = nullptr;
     Tile* d_ty = nullptr;
     Tile* d_tc = nullptr;
+    Tile* d_tr = nullptr;
     double* d_io = nullptr;      // nx*ny*6 staging for AoS transfers / rhs planes
     double* d_io2 = nullptr;
-    int n_ghosts = 0, n_heavy = 0, ntx = 0, nty = 0, ntc = 0;
+    int n_ghosts = 0, n_heavy = 0, ntx = 0, nty = 0, ntc = 0, ntr = 0;
     std::vector<int32_t> ghost_ij; // for error reports
     cudaGraphExec_t graph = nullptr;
     double graph_cfl = -1.0, graph_tfinal = 0.0;
@@ -218,7 +219,7 @@ extern "C" int rh3t_create(const rh3t_grid* grid, const rh3t_params* params, con
     }
 
     // ---- tiles
-    std::vector<Tile> tx, ty, tc;
+    std::vector<Tile> tx, ty, tc, tr;
     auto isf = [&](long i, long j) { return i >= 0 && i < nx && j >= 0 && j < ny && fluid[(size_t)i * ny + j]; };
     // x faces (i - 1/2, j), i in [0, nx]: tiles of FX_TI x FX_TJ faces
     for (long i0 = 0; i0 <= nx; i0 += FX_TI)
@@ -241,7 +242,15 @@ extern "C" int rh3t_create(const rh3t_grid* grid, const rh3t_params* params, con
             for (long j = j0; j < std::min(ny, j0 + TILE) && !any; ++j) any = isf(i, j);
             if (any) tc.push_back({0, (int)i, (int)j0, 0});
         }
-    c->ntx = (int)tx.size(); c->nty = (int)ty.size(); c->ntc = (int)tc.size();
+    // RHS / stage-update tiles: RHS_TI x RHS_TJ cells
+    for (long i0 = 0; i0 < nx; i0 += RHS_TI)
+        for (long j0 = 0; j0 < ny; j0 += RHS_TJ) {
+            bool any = false;
+            for (long i = i0; i < std::min(nx, i0 + RHS_TI) && !any; ++i)
+                for (long j = j0; j < std::min(ny, j0 + RHS_TJ) && !any; ++j) any = isf(i, j);
+            if (any) tr.push_back({0, (int)i0, (int)j0, 0});
+        }
+    c->ntx = (int)tx.size(); c->nty = (int)ty.size(); c->ntc = (int)tc.size(); c->ntr = (int)tr.size();
     I.n_tiles_dt = c->ntc;
     c->n_ghosts = ng; c->n_heavy = nh;
 
@@ -265,6 +274,7 @@ extern "C" int rh3t_create(const rh3t_grid* grid, const rh3t_params* params, con
     DA(c->d_tx, std::max(c->ntx, 1));
     DA(c->d_ty, std::max(c->nty, 1));
     DA(c->d_tc, std::max(c->ntc, 1));
+    DA(c->d_tr, std::max(c->ntr, 1));
     DA(c->d_io, nx * ny * 6);
     DA(c->d_io2, std::max((long long)nx * ny, (long long)ng) * 6); // rhs planes or ghost values
 #undef DA
@@ -306,6 +316,7 @@ extern "C" int rh3t_create(const rh3t_grid* grid, const rh3t_params* params, con
     if (c->ntx) CP(c->d_tx, tx.data(), tx.size() * sizeof(Tile));
     if (c->nty) CP(c->d_ty, ty.data(), ty.size() * sizeof(Tile));
     if (c->ntc) CP(c->d_tc, tc.data(), tc.size() * sizeof(Tile));
+    if (c->ntr) CP(c->d_tr, tr.data(), tr.size() * sizeof(Tile));
 #undef CP
     if (cudaStreamSynchronize(s) != cudaSuccess) return fail(RH3T_ERR_CUDA, "set-up synchronize failed");
     *out = c;
@@ -318,7 +329,7 @@ extern "C" void rh3t_destroy(rh3t_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->graph) cudaGraphExecDestroy(c->graph);
     void* ptrs[] = {c->d_state, c->d_mask, c->d_faces, c->d_bcs, c->d_sc, c->d_err, c->d_inst, c->d_ghosts,
-                    c->d_hst, c->d_hs, c->d_hw, c->d_hd, c->d_tx, c->d_ty, c->d_tc, c->d_io, c->d_io2};
+                    c->d_hst, c->d_hs, c->d_hw, c->d_hd, c->d_tx, c->d_ty, c->d_tc, c->d_tr, c->d_io, c->d_io2};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -363,7 +374,7 @@ static void enqueue_stage(rh3t_ctx* c, int stage) {
     cudaStream_t s = c->stream;
     launch_ghosts(s, c->d_inst, c->d_ghosts, c->n_ghosts, c->d_hst, c->d_hs, c->d_hw, c->d_hd, stage);
     launch_flux(s, c->d_inst, c->d_tx, c->ntx, c->d_ty, c->nty, stage);
-    launch_rhs_stage(s, c->d_inst, c->d_tc, c->ntc, stage, 1, nullptr);
+    launch_rhs_stage(s, c->d_inst, c->d_tr, c->ntr, stage, 1, nullptr);
     c->launches += (c->n_ghosts > 0) + 2;
 }
 
@@ -419,7 +430,7 @@ extern "C" int rh3t_l(rh3t_ctx* c, double* rhs, double* ghost_values) {
     launch_ghosts(s, c->d_inst, c->d_ghosts, c->n_ghosts, c->d_hst, c->d_hs, c->d_hw, c->d_hd, 0);
     launch_flux(s, c->d_inst, c->d_tx, c->ntx, c->d_ty, c->nty, 0);
     CK(c, cudaMemsetAsync(c->d_io2, 0, (size_t)n * 6 * sizeof(double), s));
-    launch_rhs_stage(s, c->d_inst, c->d_tc, c->ntc, 0, 0, c->d_io2);
+    launch_rhs_stage(s, c->d_inst, c->d_tr, c->ntr, 0, 0, c->d_io2);
     c->launches += 3;
     if (rhs) {
         launch_planes_to_aos(s, c->d_io2, n, c->d_io);
@@ -541,7 +552,7 @@ extern "C" int rh3t_profile_steps(rh3t_ctx* c, int32_t nsteps, double cfl_factor
             mark(0);
             launch_flux(s, c->d_inst, c->d_tx, c->ntx, c->d_ty, c->nty, st);
             mark(1);
-            launch_rhs_stage(s, c->d_inst, c->d_tc, c->ntc, st, 1, nullptr);
+            launch_rhs_stage(s, c->d_inst, c->d_tr, c->ntr, st, 1, nullptr);
             mark(2);
         }
     }

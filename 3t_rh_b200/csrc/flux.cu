@@ -1,16 +1,17 @@
 // Interface fluxes (main.rs:165-246: weno.rs:685-802 reconstruction_fast per
 // x and y face, plus diffusion.rs:27-50 when diffusion is on).
 //
-// Work split: six lanes per face, lane c owning characteristic field c
-// (5 faces per warp, lanes 30-31 only help staging). Lane c forms row c of L,
-// projects the six stencil points, runs the two WENO5 reconstructions of f+
-// and f- and obtains g_c; the six g are exchanged by warp shuffles and lane c
-// returns component c of R.g with the reference's summation order
-// (weno.rs:793, 834-843).
-//
-// Staging: a block covers 40 faces. The stencil points of the tile (x: 10x8,
-// y: 45) are loaded once into shared memory together with their physical flux
-// and the Roe inputs, instead of once per face (six times per point).
+// A block of 12 warps covers 64 faces in three phases:
+//   1. staging: the tile's stencil points (x tiles 8x8 faces -> 13x8 points,
+//      y tiles 64 faces -> 69 points) with their physical flux go to shared
+//      memory once (the reference evaluates them once per face, six times per
+//      point), and each face's Roe state and activity flag are formed once;
+//   2. characteristic pass: warp w owns characteristic field c = w % 6 for 32
+//      faces, so the row of L, the projections, the two WENO5 reconstructions
+//      of f+ and f- are warp-uniform code; g_c goes to shared memory;
+//   3. output pass: warp w owns component k = w % 6 and returns
+//      (R g)_k = sum_c R[k][c] g_c in the reference's summation order
+//      (weno.rs:793, 834-843), plus the diffusion flux for k >= 3.
 //
 // RH3T_EXACT selects the reference's expressions; otherwise the fastm forms
 // (shared reciprocals, one division per WENO5) are used.
@@ -31,134 +32,165 @@ __device__ __forceinline__ double weno5_any(double a, double b, double c, double
     return fastm::weno5(a, b, c, d, e, eps);
 }
 
+struct FluxShared {
+    double U[6][FLUX_NPT];
+    double F[6][FLUX_NPT];
+    double T[3][FLUX_NPT];
+    double Q[13][FLUX_FACES]; // Roe state per face
+    double G[6][FLUX_FACES];  // characteristic fluxes g_c per face
+    int act[FLUX_FACES];
+};
+
 template <int DIR>
-__device__ __forceinline__ void flux_tile(const Inst& I, const Tile& t, int stage, double (*sU)[FLUX_NPT],
-                                          double (*sF)[FLUX_NPT], double (*sR)[FLUX_NPT], double (*sT)[FLUX_NPT]) {
+__device__ __forceinline__ void face_index(const Tile& t, int f, int& i, int& j, int& p0, int& ps) {
+    if (DIR == 0) { i = t.i + f / FX_TJ; j = t.j0 + f % FX_TJ; p0 = f; ps = FX_TJ; }
+    else { i = t.i; j = t.j0 + f; p0 = f; ps = 1; }
+}
+
+template <int DIR>
+__device__ __forceinline__ void flux_tile(const Inst& I, const Tile& t, int stage, FluxShared& S) {
     const DevParams& P = I.P;
     const double* __restrict__ buf = stage_src(I, stage);
     const long long plane = I.plane;
     const int nx = I.nx, ny = I.ny;
     const int np = DIR == 0 ? (FX_TI + 5) * FX_TJ : FY_TJ + 5;
     const bool diff = I.diffusion != 0;
-    // ---- stage the tile's stencil points
-    for (int p = threadIdx.x; p < np; p += blockDim.x) {
-        int pi, pj;
-        if (DIR == 0) { pi = t.i - 3 + p / FX_TJ; pj = t.j0 + p % FX_TJ; }
-        else { pi = t.i; pj = t.j0 - 3 + p; }
-        double s[6] = {1.0, 0.0, 0.0, 1.0, 1.0, 1.0};
-        if (pi >= -RH3T_PAD && pi < nx + RH3T_PAD && pj >= -RH3T_PAD && pj < ny + RH3T_PAD)
-            load6(buf, plane, node_of(I, pi, pj), s);
-        Prim d = kExact ? prim_from_state(s, P) : fastm::prim(s, P);
-        double f[6];
-        phys_flux<DIR>(s, d, f);
+    // ---- 1. staging
+    for (int w = threadIdx.x; w < np + FLUX_FACES; w += blockDim.x) {
+        if (w < np) {
+            const int p = w;
+            int pi, pj;
+            if (DIR == 0) { pi = t.i - 3 + p / FX_TJ; pj = t.j0 + p % FX_TJ; }
+            else { pi = t.i; pj = t.j0 - 3 + p; }
+            double s[6] = {1.0, 0.0, 0.0, 1.0, 1.0, 1.0};
+            if (pi >= -RH3T_PAD && pi < nx + RH3T_PAD && pj >= -RH3T_PAD && pj < ny + RH3T_PAD)
+                load6(buf, plane, node_of(I, pi, pj), s);
+            Prim d = kExact ? prim_from_state(s, P) : fastm::prim(s, P);
+            double f[6];
+            phys_flux<DIR>(s, d, f);
 #pragma unroll
-        for (int k = 0; k < 6; ++k) { sU[k][p] = s[k]; sF[k][p] = f[k]; }
-        sR[0][p] = sqrt(s[0]); sR[1][p] = d.u; sR[2][p] = d.v;
-        sR[3][p] = d.e_e; sR[4][p] = d.e_i; sR[5][p] = d.e_r;
-        if (diff) {
-            double te, ti, tr;
-            temps_from_state(s, P, te, ti, tr);
-            sT[0][p] = te; sT[1][p] = ti; sT[2][p] = tr;
+            for (int k = 0; k < 6; ++k) { S.U[k][p] = s[k]; S.F[k][p] = f[k]; }
+            if (diff) {
+                double te, ti, tr;
+                temps_from_state(s, P, te, ti, tr);
+                S.T[0][p] = te; S.T[1][p] = ti; S.T[2][p] = tr;
+            }
+        } else {
+            const int f = w - np;
+            int i, j, p0, ps;
+            face_index<DIR>(t, f, i, j, p0, ps);
+            bool valid = DIR == 0 ? (i <= nx && j < ny) : (j <= ny);
+            if (valid) {
+                const uint8_t m0 = I.mask[node_of(I, i, j)];
+                const uint8_t m1 = DIR == 0 ? I.mask[node_of(I, i - 1, j)] : I.mask[node_of(I, i, j - 1)];
+                valid = (m0 | m1) != 0;
+            }
+            S.act[f] = valid ? 1 : 0;
+            if (!valid) continue;
+            double s3[6], s2[6];
+            load6(buf, plane, node_of(I, i, j), s3);
+            load6(buf, plane, DIR == 0 ? node_of(I, i - 1, j) : node_of(I, i, j - 1), s2);
+            Roe q;
+            if (kExact) {
+                const Prim d3 = prim_from_state(s3, P), d2 = prim_from_state(s2, P);
+                q = roe_average(s3[0], d3, s2[0], d2, P);
+            } else {
+                const Prim d3 = fastm::prim(s3, P), d2 = fastm::prim(s2, P);
+                const double a6[6] = {sqrt(s3[0]), d3.u, d3.v, d3.e_e, d3.e_i, d3.e_r};
+                const double b6[6] = {sqrt(s2[0]), d2.u, d2.v, d2.e_e, d2.e_i, d2.e_r};
+                q = fastm::roe(a6, b6, P);
+            }
+            const double qv[13] = {q.u, q.v, q.w2, q.ee, q.ei, q.er, q.cs2, q.cs, q.he, q.hi, q.hr, q.b, q.den};
+#pragma unroll
+            for (int k = 0; k < 13; ++k) S.Q[k][f] = qv[k];
         }
     }
     __syncthreads();
-    // ---- one face per 6 lanes
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int fw = lane < 30 ? lane / 6 : 4;
-    const int c = lane - 6 * fw;
-    const int f = warp * 5 + fw;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int c = warp % 6;                    // warp-uniform
+    const int f = (warp / 6) * 32 + lane;      // 0..63
     int i, j, p0, ps;
-    if (DIR == 0) { i = t.i + f / FX_TJ; j = t.j0 + f % FX_TJ; p0 = (f / FX_TJ) * FX_TJ + f % FX_TJ; ps = FX_TJ; }
-    else { i = t.i; j = t.j0 + f; p0 = f; ps = 1; }
-    bool active = lane < 30 && f < FLUX_FACES;
-    if (DIR == 0) active = active && i <= nx && j < ny;
-    else active = active && j <= ny;
+    face_index<DIR>(t, f, i, j, p0, ps);
+    const bool active = S.act[f] != 0;
+    auto load_q = [&](Roe& q) {
+        q.u = S.Q[0][f]; q.v = S.Q[1][f]; q.w2 = S.Q[2][f]; q.ee = S.Q[3][f]; q.ei = S.Q[4][f];
+        q.er = S.Q[5][f]; q.cs2 = S.Q[6][f]; q.cs = S.Q[7][f]; q.he = S.Q[8][f]; q.hi = S.Q[9][f];
+        q.hr = S.Q[10][f]; q.b = S.Q[11][f]; q.den = S.Q[12][f];
+    };
+    // ---- 2. characteristic pass: field c of face f
     if (active) {
-        const uint8_t m0 = I.mask[node_of(I, i, j)];
-        const uint8_t m1 = DIR == 0 ? I.mask[node_of(I, i - 1, j)] : I.mask[node_of(I, i, j - 1)];
-        active = (m0 | m1) != 0;
-    }
-    double g = 0.0, Rr[6] = {0, 0, 0, 0, 0, 0};
-    if (active) {
-        const int p2 = p0 + 2 * ps, p3 = p0 + 3 * ps;
         Roe q;
-        double a6[6], b6[6];
-#pragma unroll
-        for (int k = 0; k < 6; ++k) { a6[k] = sR[k][p3]; b6[k] = sR[k][p2]; }
-        if (kExact) {
-            Prim d3, d2;
-            d3.u = a6[1]; d3.v = a6[2]; d3.e_e = a6[3]; d3.e_i = a6[4]; d3.e_r = a6[5];
-            d2.u = b6[1]; d2.v = b6[2]; d2.e_e = b6[3]; d2.e_i = b6[4]; d2.e_r = b6[5];
-            q = roe_average(sU[0][p3], d3, sU[0][p2], d2, P);
-        } else {
-            q = fastm::roe(a6, b6, P);
-        }
-        double Lc[6], lam;
+        load_q(q);
+        double Lc[6];
         if (kExact) l_row<DIR>(c, q, P, Lc);
         else fastm::l_row<DIR>(c, q, P, Lc);
-        r_row<DIR>(c, q, P, Rr, lam);
+        const double vel = DIR == 0 ? q.u : q.v;
+        const double lam = c == 0 ? vel - q.cs : (c == 5 ? vel + q.cs : vel);
         const double a = fabs(lam);
         double fp[6], fm[6];
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
             const int p = p0 + k * ps;
-            double cf = Lc[0] * sF[0][p] + Lc[1] * sF[1][p] + Lc[2] * sF[2][p] + Lc[3] * sF[3][p] +
-                        Lc[4] * sF[4][p] + Lc[5] * sF[5][p];
-            double cs = Lc[0] * sU[0][p] + Lc[1] * sU[1][p] + Lc[2] * sU[2][p] + Lc[3] * sU[3][p] +
-                        Lc[4] * sU[4][p] + Lc[5] * sU[5][p];
+            double cf = Lc[0] * S.F[0][p] + Lc[1] * S.F[1][p] + Lc[2] * S.F[2][p] + Lc[3] * S.F[3][p] +
+                        Lc[4] * S.F[4][p] + Lc[5] * S.F[5][p];
+            double cs = Lc[0] * S.U[0][p] + Lc[1] * S.U[1][p] + Lc[2] * S.U[2][p] + Lc[3] * S.U[3][p] +
+                        Lc[4] * S.U[4][p] + Lc[5] * S.U[5][p];
             fp[k] = 0.5 * (cf + a * cs);
             fm[k] = 0.5 * (cf - a * cs);
         }
-        g = weno5_any(fp[0], fp[1], fp[2], fp[3], fp[4], P.eps) + weno5_any(fm[5], fm[4], fm[3], fm[2], fm[1], P.eps);
+        S.G[c][f] = weno5_any(fp[0], fp[1], fp[2], fp[3], fp[4], P.eps) +
+                    weno5_any(fm[5], fm[4], fm[3], fm[2], fm[1], P.eps);
     }
-    // ---- exchange g among the six lanes of the face; lane c returns (R g)_c
-    const int base = 6 * fw;
-    double gall[6];
-#pragma unroll
-    for (int k = 0; k < 6; ++k) gall[k] = __shfl_sync(0xffffffffu, g, base + k);
+    __syncthreads();
     if (!active) return;
-    double out = Rr[0] * gall[0] + Rr[1] * gall[1] + Rr[2] * gall[2] + Rr[3] * gall[3] + Rr[4] * gall[4] +
-                 Rr[5] * gall[5];
+    // ---- 3. output pass: component k = c of face f
+    const int k = c;
+    Roe q;
+    load_q(q);
+    double Rr[6], lam_unused;
+    r_row<DIR>(k, q, P, Rr, lam_unused);
+    const double out = Rr[0] * S.G[0][f] + Rr[1] * S.G[1][f] + Rr[2] * S.G[2][f] + Rr[3] * S.G[3][f] +
+                       Rr[4] * S.G[4][f] + Rr[5] * S.G[5][f];
     long long fplane, fidx;
     double *fo, *dfo;
     if (DIR == 0) { fplane = (long long)(nx + 1) * ny; fidx = (long long)i * ny + j; fo = I.fx; dfo = I.dfx; }
     else { fplane = (long long)nx * (ny + 1); fidx = (long long)i * (ny + 1) + j; fo = I.fy; dfo = I.dfy; }
-    fo[c * fplane + fidx] = out;
-    if (diff && c >= 3) {
-        // diffusion.rs:27-50: lane 3 -> ee (Te), 4 -> ei (Ti), 5 -> er (Tr^4)
-        const int k = c - 3;
+    fo[k * fplane + fidx] = out;
+    if (diff && k >= 3) {
+        // diffusion.rs:27-50: component 3 <- Te, 4 <- Ti, 5 <- Tr^4
+        const int m3 = k - 3;
         double v[6];
 #pragma unroll
         for (int m = 0; m < 6; ++m) {
-            double x = sT[k][p0 + m * ps];
-            v[m] = k == 2 ? pow4d(x) : x;
+            const double x = S.T[m3][p0 + m * ps];
+            v[m] = m3 == 2 ? pow4d(x) : x;
         }
-        const double kap = k == 0 ? P.kappa_e : (k == 1 ? P.kappa_i : P.kappa_r);
-        double term = kap * (2.0 * v[5] - 25.0 * v[4] + 245.0 * v[3] - 245.0 * v[2] + 25.0 * v[1] - 2.0 * v[0]);
-        dfo[k * fplane + fidx] = term / 180.0;
+        const double kap = m3 == 0 ? P.kappa_e : (m3 == 1 ? P.kappa_i : P.kappa_r);
+        const double term = kap * (2.0 * v[5] - 25.0 * v[4] + 245.0 * v[3] - 245.0 * v[2] + 25.0 * v[1] - 2.0 * v[0]);
+        dfo[m3 * fplane + fidx] = term / 180.0;
     }
 }
 
-__global__ void __launch_bounds__(256) k_flux(const Inst* __restrict__ insts, const Tile* __restrict__ tx, int ntx,
-                                              const Tile* __restrict__ ty, int nty, int stage) {
-    __shared__ double sU[6][FLUX_NPT], sF[6][FLUX_NPT], sR[6][FLUX_NPT], sT[3][FLUX_NPT];
+__global__ void __launch_bounds__(FLUX_THREADS) k_flux(const Inst* __restrict__ insts, const Tile* __restrict__ tx,
+                                                       int ntx, const Tile* __restrict__ ty, int nty, int stage) {
+    __shared__ FluxShared S;
     const int b = blockIdx.x;
     if (b < ntx) {
         const Tile t = tx[b];
         const Inst& I = insts[t.inst];
         if (has_error(I)) return;
-        flux_tile<0>(I, t, stage, sU, sF, sR, sT);
+        flux_tile<0>(I, t, stage, S);
     } else if (b < ntx + nty) {
         const Tile t = ty[b - ntx];
         const Inst& I = insts[t.inst];
         if (has_error(I)) return;
-        flux_tile<1>(I, t, stage, sU, sF, sR, sT);
+        flux_tile<1>(I, t, stage, S);
     }
 }
 
 void launch_flux(cudaStream_t s, const Inst* insts, const Tile* tx, int ntx, const Tile* ty, int nty, int stage) {
     if (ntx + nty <= 0) return;
-    k_flux<<<ntx + nty, 256, 0, s>>>(insts, tx, ntx, ty, nty, stage);
+    k_flux<<<ntx + nty, FLUX_THREADS, 0, s>>>(insts, tx, ntx, ty, nty, stage);
 }
 
 } // namespace rh3t

@@ -282,110 +282,6 @@ __global__ void __launch_bounds__(192) k_ghosts(const Inst* __restrict__ insts, 
     if (!fin) report(I, 1 + 2 * stage, 2, (unsigned)R.gid);
 }
 
-// ------------------------------------------------------------------ rhs + stage
-// main.rs:251-304 cell RHS fused with main.rs:308-349 stage update.
-// mode 0: write rhs to `rhs_out` (6 planes of nx*ny, i*ny+j) for l();
-// mode 1: stage update with admissibility check (main.rs:22-33).
-__device__ __forceinline__ void prim4(const double* __restrict__ buf, long long plane, long long n, const DevParams& P,
-                                      int dir, double& pe, double& pi, double& pr, double& vel) {
-    double s[6];
-    load6(buf, plane, n, s);
-    Prim d = prim_from_state(s, P);
-    pe = d.pe; pi = d.pi; pr = d.pr;
-    vel = dir == 0 ? d.u : d.v;
-}
-
-__global__ void __launch_bounds__(128) k_rhs_stage(const Inst* __restrict__ insts, const Tile* __restrict__ tiles,
-                                                   int nt, int stage, int mode, double* __restrict__ rhs_out) {
-    if (blockIdx.x >= nt) return;
-    const Tile t = tiles[blockIdx.x];
-    const Inst& I = insts[t.inst];
-    const int i = t.i, j = t.j0 + threadIdx.x;
-    if (j >= I.ny || has_error(I)) return;
-    const long long n = node_of(I, i, j);
-    if (!I.mask[n]) return;
-    const DevParams& P = I.P;
-    const long long plane = I.plane;
-    const double* __restrict__ src = stage_src(I, stage);
-    const double dx = I.dx, dy = I.dy;
-    const long long fpx = (long long)(I.nx + 1) * I.ny, fix = (long long)i * I.ny + j;
-    const long long fpy = (long long)I.nx * (I.ny + 1), fiy = (long long)i * (I.ny + 1) + j;
-    double rhs[6];
-    const double sx = 1.0 / dx, sy = 1.0 / dy;
-#pragma unroll
-    for (int c = 0; c < 6; ++c) {
-        double fl = I.fx[c * fpx + fix], fr = I.fx[c * fpx + fix + I.ny];
-        double fb = I.fy[c * fpy + fiy], ft = I.fy[c * fpy + fiy + 1];
-        rhs[c] = -(fr - fl) * sx + -(ft - fb) * sy;
-    }
-    double pe[9], pi[9], pr[9], vel[9], ncx[3], ncy[3];
-#pragma unroll
-    for (int q = 0; q < 9; ++q) prim4(src, plane, node_of(I, i - 4 + q, j), P, 0, pe[q], pi[q], pr[q], vel[q]);
-    noncon9(pe, pi, pr, vel, dx, ncx);
-#pragma unroll
-    for (int q = 0; q < 9; ++q) prim4(src, plane, node_of(I, i, j - 4 + q), P, 1, pe[q], pi[q], pr[q], vel[q]);
-    noncon9(pe, pi, pr, vel, dy, ncy);
-    double add[3] = {ncx[0], ncx[1], ncx[2]};
-#pragma unroll
-    for (int k = 0; k < 3; ++k) rhs[3 + k] = rhs[3 + k] + add[k] + ncy[k];
-    if (I.source) {
-        // source.rs:7-21
-        double s[6];
-        load6(src, plane, n, s);
-        double te, ti, tr;
-        temps_from_state(s, P, te, ti, tr);
-        double so[3] = {-P.omega_ei * (te - ti) - P.omega_er * (pow4d(te) - pow4d(tr)), P.omega_ei * (te - ti),
-                        P.omega_er * (pow4d(te) - pow4d(tr))};
-#pragma unroll
-        for (int k = 0; k < 3; ++k) rhs[3 + k] = rhs[3 + k] + so[k];
-    }
-    if (I.diffusion) {
-        const double cx = -1.0 / (dx * dx), cy = -1.0 / (dy * dy);
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            double a = I.dfx[k * fpx + fix], b = I.dfx[k * fpx + fix + I.ny];
-            double c2 = I.dfy[k * fpy + fiy], d2 = I.dfy[k * fpy + fiy + 1];
-            rhs[3 + k] = rhs[3 + k] + ((-(b - a) * cx) + (-(d2 - c2) * cy));
-        }
-    }
-    if (mode == 0) {
-        const long long ln = (long long)i * I.ny + j, lp = (long long)I.nx * I.ny;
-#pragma unroll
-        for (int c = 0; c < 6; ++c) rhs_out[c * lp + ln] = rhs[c];
-        return;
-    }
-    const DevScalars& sc = *I.sc;
-    double v[6];
-    if (stage == 0) {
-        const double coef = sc.coef[0];
-#pragma unroll
-        for (int c = 0; c < 6; ++c) v[c] = I.U[c * plane + n] + rhs[c] * coef;
-#pragma unroll
-        for (int c = 0; c < 6; ++c) I.A[c * plane + n] = v[c];
-    } else if (stage == 1) {
-        const double coef = sc.coef[1];
-#pragma unroll
-        for (int c = 0; c < 6; ++c) v[c] = I.U[c * plane + n] * 0.75 + I.A[c * plane + n] * 0.25 + rhs[c] * coef;
-#pragma unroll
-        for (int c = 0; c < 6; ++c) I.B[c * plane + n] = v[c];
-    } else {
-        const double coef = sc.coef[2];
-        const double wb = 1.0 / 3.0, wa = 2.0 / 3.0;
-#pragma unroll
-        for (int c = 0; c < 6; ++c) v[c] = I.U[c * plane + n] * wb + I.B[c * plane + n] * wa + rhs[c] * coef;
-#pragma unroll
-        for (int c = 0; c < 6; ++c) I.U[c * plane + n] = v[c];
-    }
-    bool ok = isfinite(v[0]) && isfinite(v[1]) && isfinite(v[2]) && isfinite(v[3]) && isfinite(v[4]) &&
-              isfinite(v[5]) && v[0] > 0.0;
-    if (ok) {
-        double ux = v[1] / v[0], uy = v[2] / v[0];
-        double k = (ux * ux + uy * uy) / 6.0;
-        ok = !(v[3] / v[0] - k <= 0.0 || v[4] / v[0] - k <= 0.0 || v[5] / v[0] - k <= 0.0);
-    }
-    if (!ok) report(I, 2 + 2 * stage, 1, (unsigned)((long long)i * I.ny + j));
-}
-
 // ------------------------------------------------------------------ dt
 // Orderable 64-bit key of a double (total order, NaN excluded by the caller).
 __device__ __forceinline__ unsigned long long dkey(double x) {
@@ -567,10 +463,6 @@ void launch_ghosts(cudaStream_t s, const Inst* insts, const GhostRec* recs, int 
     if (n <= 0) return;
     dim3 blk(6, 32);
     k_ghosts<<<(n + 31) / 32, blk, 0, s>>>(insts, recs, n, hst, hs, hw, hd, stage);
-}
-void launch_rhs_stage(cudaStream_t s, const Inst* insts, const Tile* tc, int nt, int stage, int mode, double* rhs) {
-    if (nt <= 0) return;
-    k_rhs_stage<<<nt, 128, 0, s>>>(insts, tc, nt, stage, mode, rhs);
 }
 void launch_dt(cudaStream_t s, const Inst* insts, const Tile* tc, int nt, int mode) {
     if (nt <= 0) return;

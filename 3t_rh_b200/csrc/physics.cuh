@@ -510,4 +510,31 @@ __device__ __forceinline__ double local_dt(const double s[6], double dx, double 
     return P.lambda / vj;
 }
 
+namespace fastm {
+
+// noncon.rs:288-332 with the divisions by 60 ds, 3 and ds as multiplications
+__device__ __forceinline__ void noncon9(const double pe[9], const double pi[9], const double pr[9],
+                                        const double vel[9], double inv_60ds, double inv_ds, double out[3]) {
+    const double v = vel[4];
+    auto d6f = [&](const double* q) {
+        return (q[7] - 9.0 * q[6] + 45.0 * q[5] - 45.0 * q[3] + 9.0 * q[2] - q[1]) * inv_60ds;
+    };
+    const double dpe = d6f(pe), dpi = d6f(pi), dpr = d6f(pr);
+    const double der[3] = {2.0 * dpe - dpi - dpr, 2.0 * dpi - dpe - dpr, 2.0 * dpr - dpe - dpi};
+    double n[3][9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        n[0][k] = 2.0 * pe[k] - pi[k] - pr[k];
+        n[1][k] = 2.0 * pi[k] - pe[k] - pr[k];
+        n[2][k] = 2.0 * pr[k] - pe[k] - pi[k];
+    }
+    const double cl = fmax(fmax(v, vel[3]), 0.0) * (1.0 / 3.0) * inv_ds;
+    const double cr = fmin(fmin(v, vel[5]), 0.0) * (1.0 / 3.0) * inv_ds;
+    const double v3 = v * (1.0 / 3.0);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) out[c] = v3 * der[c] + (cl * jump8(n[c]) + cr * jump8(n[c] + 1));
+}
+
+} // namespace fastm
+
 } // namespace rh3t

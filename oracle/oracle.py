@@ -15,6 +15,18 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
 _lib = None
 
+
+def fma_variant():
+    """A second instance of this module bound to liboracle_fma.so (the
+    restatement compiled with FMA contraction): the rounding envelope of the
+    reference algorithm."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("oracle_fma_variant", os.path.abspath(__file__))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    mod._LIB_PATH = os.path.join(_HERE, "_build", "liboracle_fma.so")
+    return mod
+
 # Order of the 15 runtime parameters (oracle/src/physics.hpp Params)
 PARAM_NAMES = ("gamma_e", "gamma_i", "gamma_r", "cve", "cvi", "a_rad", "kappa_e", "kappa_i", "kappa_r",
                "omega_ei", "omega_er", "lambda_", "weno_q", "eps", "periodic_ly")

@@ -77,8 +77,14 @@ def test_rk3_cylinder_100_steps(rh, O, exact, tol):
     assert abs(s.last_dt() - dts[-1]) <= 1e-10 * dts[-1]
 
 
-@pytest.mark.parametrize("exact,tol", [(True, 1e-10), (False, 1e-10)])
-def test_planar_shock_periodic_outflow_diffusion_source(rh, O, exact, tol):
+@pytest.mark.parametrize("exact", [True, False])
+def test_planar_shock_periodic_outflow_diffusion_source(rh, O, exact):
+    """With diffusion and exchange both on, the corner ghosts where the
+    reference picks FarField over Periodic (ghost.rs:285-348) seed a transverse
+    momentum that amplifies any rounding difference: the oracle compiled with
+    FMA contraction differs from itself without by ~1e-9 after 100 steps. The
+    exact build must match the oracle to 1e-10 (it is bit-identical in
+    practice); the FMA build must stay within 1e-10 or within that envelope."""
     f, g, ref = _pair(rh, O, "planar")
     s = rh.Solver(f, g, exact=exact)
     s.advance(100, 0.05)
@@ -86,7 +92,15 @@ def test_planar_shock_periodic_outflow_diffusion_source(rh, O, exact, tol):
     u, _ = s.download()
     err = rel_linf(u, ref.state(), f.fluid)
     print(f"planar shock 1024x8 100 steps exact={exact}: per-field {err}")
-    assert err.max() <= tol
+    if exact:
+        assert err.max() <= 1e-10
+    else:
+        p = dict(kappa_e=1e-3, kappa_i=1e-3, kappa_r=1e-3, omega_ei=1.0, omega_er=1.0, periodic_ly=0.03125)
+        ref_fma = O.fma_variant().Case.planar_shock(**p)
+        ref_fma.run(100, 0.05)
+        env = rel_linf(ref_fma.state(), ref.state(), f.fluid).max()
+        print(f"  oracle FMA-vs-plain envelope {env:.3e}")
+        assert err.max() <= max(1e-10, env)
 
 
 def test_graph_and_eager_identical(rh, O):
