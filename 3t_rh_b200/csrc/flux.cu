@@ -1,17 +1,20 @@
 // Interface fluxes (main.rs:165-246: weno.rs:685-802 reconstruction_fast per
 // x and y face, plus diffusion.rs:27-50 when diffusion is on).
 //
-// A block of 12 warps covers 64 faces in three phases:
+// A block of 6 warps covers 64 faces in three phases:
 //   1. staging: the tile's stencil points (x tiles 8x8 faces -> 13x8 points,
 //      y tiles 64 faces -> 69 points) with their physical flux go to shared
 //      memory once (the reference evaluates them once per face, six times per
 //      point), and each face's Roe state and activity flag are formed once;
-//   2. characteristic pass: warp w owns characteristic field c = w % 6 for 32
-//      faces, so the row of L, the projections, the two WENO5 reconstructions
-//      of f+ and f- are warp-uniform code; g_c goes to shared memory;
-//   3. output pass: warp w owns component k = w % 6 and returns
+//   2. characteristic pass: warp c owns characteristic field c for the 64
+//      faces (two per lane), so the row of L, the projections and the two
+//      WENO5 reconstructions of f+ and f- are warp-uniform code; g_c goes to
+//      shared memory;
+//   3. output pass: warp k owns component k and returns
 //      (R g)_k = sum_c R[k][c] g_c in the reference's summation order
 //      (weno.rs:793, 834-843), plus the diffusion flux for k >= 3.
+// Point data sit in shared memory as component pairs (double2), so a lane
+// reads a point's state and flux with six 16-byte loads.
 //
 // RH3T_EXACT selects the reference's expressions; otherwise the fastm forms
 // (shared reciprocals, one division per WENO5) are used.
@@ -32,12 +35,14 @@ __device__ __forceinline__ double weno5_any(double a, double b, double c, double
     return fastm::weno5(a, b, c, d, e, eps);
 }
 
+constexpr int NQ = 15; // Roe state: u v w2 ee ei er cs2 cs he hi hr b den, 1/cs2, 1/b
+
 struct FluxShared {
-    double U[6][FLUX_NPT];
-    double F[6][FLUX_NPT];
+    double2 U[3][FLUX_NPT]; // (rho, mx), (my, ee), (ei, er)
+    double2 F[3][FLUX_NPT];
     double T[3][FLUX_NPT];
-    double Q[13][FLUX_FACES]; // Roe state per face
-    double G[6][FLUX_FACES];  // characteristic fluxes g_c per face
+    double Q[NQ][FLUX_FACES];
+    double G[6][FLUX_FACES];
     int act[FLUX_FACES];
 };
 
@@ -45,6 +50,73 @@ template <int DIR>
 __device__ __forceinline__ void face_index(const Tile& t, int f, int& i, int& j, int& p0, int& ps) {
     if (DIR == 0) { i = t.i + f / FX_TJ; j = t.j0 + f % FX_TJ; p0 = f; ps = FX_TJ; }
     else { i = t.i; j = t.j0 + f; p0 = f; ps = 1; }
+}
+
+__device__ __forceinline__ void load_q(const FluxShared& S, int f, Roe& q, double& ics2, double& ib) {
+    q.u = S.Q[0][f]; q.v = S.Q[1][f]; q.w2 = S.Q[2][f]; q.ee = S.Q[3][f]; q.ei = S.Q[4][f];
+    q.er = S.Q[5][f]; q.cs2 = S.Q[6][f]; q.cs = S.Q[7][f]; q.he = S.Q[8][f]; q.hi = S.Q[9][f];
+    q.hr = S.Q[10][f]; q.b = S.Q[11][f]; q.den = S.Q[12][f];
+    ics2 = S.Q[13][f]; ib = S.Q[14][f];
+}
+
+template <int DIR>
+__device__ __forceinline__ double char_flux(const FluxShared& S, const DevParams& P, int c, int f, int p0, int ps) {
+    Roe q;
+    double ics2, ib;
+    load_q(S, f, q, ics2, ib);
+    double Lc[6];
+    if (kExact) l_row<DIR>(c, q, P, Lc);
+    else fastm::l_row<DIR>(c, q, ics2, ib, P, Lc);
+    const double vel = DIR == 0 ? q.u : q.v;
+    const double lam = c == 0 ? vel - q.cs : (c == 5 ? vel + q.cs : vel);
+    const double a = fabs(lam);
+    double fp[6], fm[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        const int p = p0 + k * ps;
+        const double2 u01 = S.U[0][p], u23 = S.U[1][p], u45 = S.U[2][p];
+        const double2 f01 = S.F[0][p], f23 = S.F[1][p], f45 = S.F[2][p];
+        const double cf = Lc[0] * f01.x + Lc[1] * f01.y + Lc[2] * f23.x + Lc[3] * f23.y + Lc[4] * f45.x +
+                          Lc[5] * f45.y;
+        const double cs = Lc[0] * u01.x + Lc[1] * u01.y + Lc[2] * u23.x + Lc[3] * u23.y + Lc[4] * u45.x +
+                          Lc[5] * u45.y;
+        fp[k] = 0.5 * (cf + a * cs);
+        fm[k] = 0.5 * (cf - a * cs);
+    }
+    return weno5_any(fp[0], fp[1], fp[2], fp[3], fp[4], P.eps) + weno5_any(fm[5], fm[4], fm[3], fm[2], fm[1], P.eps);
+}
+
+template <int DIR>
+__device__ __forceinline__ void face_out(const Inst& I, const FluxShared& S, const Tile& t, int k, int f) {
+    const DevParams& P = I.P;
+    const int nx = I.nx, ny = I.ny;
+    int i, j, p0, ps;
+    face_index<DIR>(t, f, i, j, p0, ps);
+    Roe q;
+    double ics2, ib;
+    load_q(S, f, q, ics2, ib);
+    double Rr[6], lam_unused;
+    r_row<DIR>(k, q, P, Rr, lam_unused);
+    const double out = Rr[0] * S.G[0][f] + Rr[1] * S.G[1][f] + Rr[2] * S.G[2][f] + Rr[3] * S.G[3][f] +
+                       Rr[4] * S.G[4][f] + Rr[5] * S.G[5][f];
+    long long fplane, fidx;
+    double *fo, *dfo;
+    if (DIR == 0) { fplane = (long long)(nx + 1) * ny; fidx = (long long)i * ny + j; fo = I.fx; dfo = I.dfx; }
+    else { fplane = (long long)nx * (ny + 1); fidx = (long long)i * (ny + 1) + j; fo = I.fy; dfo = I.dfy; }
+    fo[k * fplane + fidx] = out;
+    if (I.diffusion && k >= 3) {
+        // diffusion.rs:27-50: component 3 <- Te, 4 <- Ti, 5 <- Tr^4
+        const int m3 = k - 3;
+        double v[6];
+#pragma unroll
+        for (int m = 0; m < 6; ++m) {
+            const double x = S.T[m3][p0 + m * ps];
+            v[m] = m3 == 2 ? pow4d(x) : x;
+        }
+        const double kap = m3 == 0 ? P.kappa_e : (m3 == 1 ? P.kappa_i : P.kappa_r);
+        const double term = kap * (2.0 * v[5] - 25.0 * v[4] + 245.0 * v[3] - 245.0 * v[2] + 25.0 * v[1] - 2.0 * v[0]);
+        dfo[m3 * fplane + fidx] = term / 180.0;
+    }
 }
 
 template <int DIR>
@@ -69,7 +141,10 @@ __device__ __forceinline__ void flux_tile(const Inst& I, const Tile& t, int stag
             double f[6];
             phys_flux<DIR>(s, d, f);
 #pragma unroll
-            for (int k = 0; k < 6; ++k) { S.U[k][p] = s[k]; S.F[k][p] = f[k]; }
+            for (int k = 0; k < 3; ++k) {
+                S.U[k][p] = make_double2(s[2 * k], s[2 * k + 1]);
+                S.F[k][p] = make_double2(f[2 * k], f[2 * k + 1]);
+            }
             if (diff) {
                 double te, ti, tr;
                 temps_from_state(s, P, te, ti, tr);
@@ -100,74 +175,30 @@ __device__ __forceinline__ void flux_tile(const Inst& I, const Tile& t, int stag
                 const double b6[6] = {sqrt(s2[0]), d2.u, d2.v, d2.e_e, d2.e_i, d2.e_r};
                 q = fastm::roe(a6, b6, P);
             }
-            const double qv[13] = {q.u, q.v, q.w2, q.ee, q.ei, q.er, q.cs2, q.cs, q.he, q.hi, q.hr, q.b, q.den};
+            const double qv[NQ] = {q.u, q.v, q.w2, q.ee, q.ei, q.er, q.cs2, q.cs, q.he, q.hi, q.hr, q.b, q.den,
+                                   kExact ? 0.0 : 1.0 / q.cs2, kExact ? 0.0 : 1.0 / q.b};
 #pragma unroll
-            for (int k = 0; k < 13; ++k) S.Q[k][f] = qv[k];
+            for (int k = 0; k < NQ; ++k) S.Q[k][f] = qv[k];
         }
     }
     __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int c = warp % 6;                    // warp-uniform
-    const int f = (warp / 6) * 32 + lane;      // 0..63
-    int i, j, p0, ps;
-    face_index<DIR>(t, f, i, j, p0, ps);
-    const bool active = S.act[f] != 0;
-    auto load_q = [&](Roe& q) {
-        q.u = S.Q[0][f]; q.v = S.Q[1][f]; q.w2 = S.Q[2][f]; q.ee = S.Q[3][f]; q.ei = S.Q[4][f];
-        q.er = S.Q[5][f]; q.cs2 = S.Q[6][f]; q.cs = S.Q[7][f]; q.he = S.Q[8][f]; q.hi = S.Q[9][f];
-        q.hr = S.Q[10][f]; q.b = S.Q[11][f]; q.den = S.Q[12][f];
-    };
-    // ---- 2. characteristic pass: field c of face f
-    if (active) {
-        Roe q;
-        load_q(q);
-        double Lc[6];
-        if (kExact) l_row<DIR>(c, q, P, Lc);
-        else fastm::l_row<DIR>(c, q, P, Lc);
-        const double vel = DIR == 0 ? q.u : q.v;
-        const double lam = c == 0 ? vel - q.cs : (c == 5 ? vel + q.cs : vel);
-        const double a = fabs(lam);
-        double fp[6], fm[6];
+    const int c = threadIdx.x >> 5, lane = threadIdx.x & 31; // warp-uniform characteristic field
+    // ---- 2. characteristic pass: field c of faces lane and lane + 32
 #pragma unroll
-        for (int k = 0; k < 6; ++k) {
-            const int p = p0 + k * ps;
-            double cf = Lc[0] * S.F[0][p] + Lc[1] * S.F[1][p] + Lc[2] * S.F[2][p] + Lc[3] * S.F[3][p] +
-                        Lc[4] * S.F[4][p] + Lc[5] * S.F[5][p];
-            double cs = Lc[0] * S.U[0][p] + Lc[1] * S.U[1][p] + Lc[2] * S.U[2][p] + Lc[3] * S.U[3][p] +
-                        Lc[4] * S.U[4][p] + Lc[5] * S.U[5][p];
-            fp[k] = 0.5 * (cf + a * cs);
-            fm[k] = 0.5 * (cf - a * cs);
+    for (int h = 0; h < FLUX_FACES / 32; ++h) {
+        const int f = lane + 32 * h;
+        if (S.act[f]) {
+            int i, j, p0, ps;
+            face_index<DIR>(t, f, i, j, p0, ps);
+            S.G[c][f] = char_flux<DIR>(S, P, c, f, p0, ps);
         }
-        S.G[c][f] = weno5_any(fp[0], fp[1], fp[2], fp[3], fp[4], P.eps) +
-                    weno5_any(fm[5], fm[4], fm[3], fm[2], fm[1], P.eps);
     }
     __syncthreads();
-    if (!active) return;
-    // ---- 3. output pass: component k = c of face f
-    const int k = c;
-    Roe q;
-    load_q(q);
-    double Rr[6], lam_unused;
-    r_row<DIR>(k, q, P, Rr, lam_unused);
-    const double out = Rr[0] * S.G[0][f] + Rr[1] * S.G[1][f] + Rr[2] * S.G[2][f] + Rr[3] * S.G[3][f] +
-                       Rr[4] * S.G[4][f] + Rr[5] * S.G[5][f];
-    long long fplane, fidx;
-    double *fo, *dfo;
-    if (DIR == 0) { fplane = (long long)(nx + 1) * ny; fidx = (long long)i * ny + j; fo = I.fx; dfo = I.dfx; }
-    else { fplane = (long long)nx * (ny + 1); fidx = (long long)i * (ny + 1) + j; fo = I.fy; dfo = I.dfy; }
-    fo[k * fplane + fidx] = out;
-    if (diff && k >= 3) {
-        // diffusion.rs:27-50: component 3 <- Te, 4 <- Ti, 5 <- Tr^4
-        const int m3 = k - 3;
-        double v[6];
+    // ---- 3. output pass: component k = c
 #pragma unroll
-        for (int m = 0; m < 6; ++m) {
-            const double x = S.T[m3][p0 + m * ps];
-            v[m] = m3 == 2 ? pow4d(x) : x;
-        }
-        const double kap = m3 == 0 ? P.kappa_e : (m3 == 1 ? P.kappa_i : P.kappa_r);
-        const double term = kap * (2.0 * v[5] - 25.0 * v[4] + 245.0 * v[3] - 245.0 * v[2] + 25.0 * v[1] - 2.0 * v[0]);
-        dfo[m3 * fplane + fidx] = term / 180.0;
+    for (int h = 0; h < FLUX_FACES / 32; ++h) {
+        const int f = lane + 32 * h;
+        if (S.act[f]) face_out<DIR>(I, S, t, c, f);
     }
 }
 

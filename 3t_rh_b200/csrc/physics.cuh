@@ -346,13 +346,14 @@ __device__ __forceinline__ Roe roe(const double a[6], const double b[6], const D
     return q;
 }
 
+// ics2 = 1 / cs2 and ib = 1 / b of the face (formed once per face)
 template <int DIR>
-__device__ __forceinline__ void l_row(int row, const Roe& q, const DevParams& P, double L[6]) {
+__device__ __forceinline__ void l_row(int row, const Roe& q, double ics2, double ib, const DevParams& P,
+                                      double L[6]) {
     const double GE = P.gamma_e, GI = P.gamma_i, GR = P.gamma_r;
     const double gi = GI - 1.0, ge = GE - 1.0, gr = GR - 1.0;
     const double gt = gi + ge + gr;
     const double u = q.u, v = q.v, w2 = q.w2, cs = q.cs, cs2 = q.cs2;
-    const double ics2 = 1.0 / cs2, ib = 1.0 / q.b;
     const double iden = ics2 * (1.0 / 12.0);
     int mode;
     if (DIR == 0) {

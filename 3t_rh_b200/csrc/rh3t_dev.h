@@ -110,7 +110,7 @@ constexpr int CELL_TILE = 128;
 constexpr int RHS_TI = 8, RHS_TJ = 32;           // RHS/stage tiles: RHS_TI x RHS_TJ cells
 constexpr int FX_TI = 8, FX_TJ = 8, FY_TJ = 64;
 constexpr int FLUX_FACES = 64;                   // faces per flux block
-constexpr int FLUX_THREADS = 384;                // 12 warps: 6 characteristic fields x 2 groups of 32 faces
+constexpr int FLUX_THREADS = 192;                // 6 warps: one per characteristic field
 constexpr int FLUX_NPT = (FX_TI + 5) * FX_TJ;    // staged points per flux block (>= FY_TJ + 5)
 
 } // namespace rh3t
