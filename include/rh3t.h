@@ -180,6 +180,25 @@ int rh3t_l(rh3t_ctx* ctx, double* rhs, double* ghost_values);
 /* main.rs:375-408 calc_global_dt of the resident state */
 int rh3t_calc_global_dt(rh3t_ctx* ctx, double* dt_cfl);
 
+/* Allocation-free calc_global_dt for callers that cannot allocate device
+ * memory (a host framework or pool owns all device memory, or an allocation
+ * would synchronise the device at that point). No counterpart in the
+ * reference (it is a variant of rh3t_calc_global_dt for such callers).
+ * d_value: device array of nx*ny records of 6 doubles (i*ny + j), d_fluid:
+ * device nx*ny bytes, d_dt_cfl: device double receiving the minimum; the work
+ * is queued on `stream` (a cudaStream_t, NULL = default stream) and nothing is
+ * allocated or freed. The scratch (one partial minimum per 256 nodes) is a
+ * static device array of RH3T_DT_NOALLOC_MAX_CELLS / 256 doubles (512 KiB)
+ * that every GPU loading the library keeps until exit: grids of more than
+ * RH3T_DT_NOALLOC_MAX_CELLS nodes are rejected with
+ * RH3T_ERR_INVALID_ARGUMENT. The first call on a device looks the array's
+ * address up (cudaGetSymbolAddress): make it before any stream capture. All
+ * calls share the array, so calls that overlap on the GPU race; calls
+ * ordered on one stream are safe (each writes every entry it reads). */
+#define RH3T_DT_NOALLOC_MAX_CELLS (65536 * 256)
+int rh3t_calc_global_dt_noalloc(const rh3t_grid* grid, const rh3t_params* params, const double* d_value,
+                                const uint8_t* d_fluid, double* d_dt_cfl, void* stream);
+
 /* main.rs:351-373 rk3_ssp with a caller-given dt, resident state */
 int rh3t_rk3_ssp(rh3t_ctx* ctx, double dt);
 
