@@ -98,6 +98,21 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
+def replica_value(ms_local, cells_local, steps, dist=None, device="cpu"):
+    """Whole-job cell-updates/s of independent replicas: the sum of all ranks'
+    cell-updates over the slowest rank's time (MAX all-reduce of the device
+    times, SUM of the cells). Returns (value, max_ms)."""
+    import torch
+    if dist is None:
+        return cells_local * steps / (ms_local * 1e-3), ms_local
+    t = torch.tensor([ms_local], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    c = torch.tensor([float(cells_local)], dtype=torch.float64, device=device)
+    dist.all_reduce(c, op=dist.ReduceOp.SUM)
+    ms = float(t.item())
+    return float(c.item()) * steps / (ms * 1e-3), ms
+
+
 def cpu_baseline(O, wl, budget_s=20.0):
     """The oracle (OpenMP, all host threads) on a bounded number of steps of the same workload."""
     t0 = time.perf_counter()
@@ -211,13 +226,9 @@ def main():
     torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1)
     launches = s.kernel_launches - l0
-    if dist:
-        t = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    value, ms = replica_value(ms, cells, args.steps, dist, f"cuda:{local}")
     sampler.stop()
     clocks = sampler.summary()
-    value = world * cells * args.steps / (ms * 1e-3)
 
     # roofline of the dominant kernel: live per-launch durations (CUDA events)
     prof = s.profile_steps(min(args.steps, 20), CFL)
