@@ -37,6 +37,10 @@ WORKLOADS = {
 }
 PLANAR_PARAMS = dict(kappa_e=1e-3, kappa_i=1e-3, kappa_r=1e-3, omega_ei=1.0, omega_er=1.0, periodic_ly=0.03125)
 CFL = 0.05
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_flux
+# launch, from an ncu capture of `bench.py --steps 3 --warmup 3 --no-cpu
+# --no-e2e` (FMA build); None where no capture exists
+FLUX_TRAFFIC_BYTES = {"cyl961": 651.5e6}
 
 
 def make_field(rh, wl):
@@ -273,7 +277,9 @@ def main():
                        "arithmetic": "no FMA contraction" if args.exact else "FMA contraction",
                        "ghost_build_s": round(build_s, 3)},
             "roofline": {"bound": "fp64", "kernel": "k_flux (x+y interface WENO5 fluxes)", "achieved": achieved,
-                         "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                         "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                         "traffic": None if args.exact else FLUX_TRAFFIC_BYTES.get(args.workload),
+                         "traffic_unit": "bytes per launch",
                          "peak_source": "measured DFMA loop on this GPU (rh3t_fp64_peak)",
                          "flops_per_launch": fl_launch, "launch_ms": flux_ms / flux_n,
                          "kernel_share": {k: v[0] / total_prof_ms for k, v in prof.items()},

@@ -103,6 +103,26 @@ def test_planar_shock_periodic_outflow_diffusion_source(rh, O, exact):
         assert err.max() <= max(1e-10, env)
 
 
+@pytest.mark.parametrize("exact", [True, False])
+def test_double_mach_wall_ilw(rh, O, exact):
+    """init_double_mach (init.rs:26-113): the only reference case with Wall
+    (ILW rows + two 6x6 LU solves per ghost, bc1.rs:691-756), Constant and
+    ZerothOrder ghosts; h = 1/80 (220 x 159 nodes), 20 steps."""
+    f, g, ref = _pair(rh, O, "dmr", h=1.0 / 80.0)
+    s = rh.Solver(f, g, exact=exact)
+    rhs, gv = s.l(with_ghosts=True)
+    rr, rg = ref.l()
+    e_l = rel_linf(gv, rg, np.ones(len(rg), bool)).max()
+    s.advance(20, 0.05)
+    ref.run(20, 0.05)
+    u, _ = s.download()
+    err = rel_linf(u, ref.state(), f.fluid)
+    print(f"double Mach 20 steps exact={exact}: ghosts of l() {e_l:.3e}, state per-field {err}")
+    assert err.max() <= 1e-10
+    if exact:
+        assert e_l <= 1e-13
+
+
 def test_graph_and_eager_identical(rh, O):
     f, g, _ = _pair(rh, O)
     a = rh.Solver(f, g)
