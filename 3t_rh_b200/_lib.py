@@ -10,6 +10,7 @@ RH3T_OK = 0
 STATUS_NAMES = {
     0: "OK", 1: "NONPHYSICAL_STATE", 2: "NONFINITE_GHOST", 3: "SINGULAR_ILW", 4: "PERIODIC_WRAP",
     5: "STENCIL_FIT", 6: "GEOMETRY", 7: "INVALID_ARGUMENT", 8: "CUDA", 9: "NONPOSITIVE_DT", 10: "NO_DEVICE",
+    11: "DEVICE_TIMEOUT",
 }
 
 # exported symbols of include/rh3t.h
@@ -17,8 +18,12 @@ EXPORTS = (
     "rh3t_geom_create", "rh3t_geom_fluid_mask", "rh3t_geom_build_ghosts", "rh3t_geom_ghost_table",
     "rh3t_geom_access_table", "rh3t_geom_last_error", "rh3t_geom_destroy", "rh3t_default_params", "rh3t_create",
     "rh3t_upload_state", "rh3t_download_state", "rh3t_l", "rh3t_calc_global_dt", "rh3t_rk3_ssp", "rh3t_advance",
-    "rh3t_step_host", "rh3t_last_dt", "rh3t_profile_steps", "rh3t_fp64_peak", "rh3t_math_check", "rh3t_calc_global_dt_noalloc", "rh3t_synchronize", "rh3t_last_error", "rh3t_kernel_launches", "rh3t_stream",
-    "rh3t_destroy",
+    "rh3t_step_host", "rh3t_last_dt", "rh3t_profile_steps", "rh3t_fp64_peak", "rh3t_math_check",
+    "rh3t_calc_global_dt_noalloc", "rh3t_synchronize", "rh3t_last_error", "rh3t_kernel_launches", "rh3t_stream",
+    "rh3t_destroy", "rh3t_batch_create", "rh3t_instance_count", "rh3t_upload_batch", "rh3t_download_batch",
+    "rh3t_upload_instance", "rh3t_download_instance", "rh3t_l_instance", "rh3t_calc_global_dt_batch",
+    "rh3t_instance_times", "rh3t_instance_status", "rh3t_set_tile_shapes", "rh3t_get_tile_shapes",
+    "rh3t_autotune",
 )
 
 
@@ -55,7 +60,19 @@ class GhostTable(C.Structure):
 
 class Error(C.Structure):
     _fields_ = [("code", C.c_int32), ("stage", C.c_int32), ("step", C.c_int64), ("i", C.c_int32),
-                ("j", C.c_int32), ("ghost", C.c_int32), ("message", C.c_char * 160)]
+                ("j", C.c_int32), ("ghost", C.c_int32), ("instance", C.c_int32), ("message", C.c_char * 160)]
+
+
+class Instance(C.Structure):
+    _fields_ = [("grid", C.c_void_p), ("params", C.c_void_p), ("fluid", C.c_void_p), ("n_outer_bc", C.c_int32),
+                ("outer_bcs", C.c_void_p), ("n_inner_bc", C.c_int32), ("inner_bcs", C.c_void_p),
+                ("ghosts", C.c_void_p)]
+
+
+class TuneEntry(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("diffusion", C.c_int32), ("n_instances", C.c_int32),
+                ("lg_fx", C.c_int32), ("lg_fy", C.c_int32), ("lg_rhs", C.c_int32), ("from_cache", C.c_int32),
+                ("ms_fx", C.c_double * 3), ("ms_fy", C.c_double * 3), ("ms_rhs", C.c_double * 3)]
 
 
 _libs = {}
@@ -103,6 +120,19 @@ def load(exact=False):
         "rh3t_kernel_launches": (C.c_int64, [V]),
         "rh3t_stream": (V, [V]),
         "rh3t_destroy": (None, [V]),
+        "rh3t_batch_create": (I, [C.c_int32, V, C.c_int32, P(V)]),
+        "rh3t_instance_count": (C.c_int32, [V]),
+        "rh3t_upload_batch": (I, [V, V, V]),
+        "rh3t_download_batch": (I, [V, V, V]),
+        "rh3t_upload_instance": (I, [V, C.c_int32, V, D]),
+        "rh3t_download_instance": (I, [V, C.c_int32, V, P(D)]),
+        "rh3t_l_instance": (I, [V, C.c_int32, V, V]),
+        "rh3t_calc_global_dt_batch": (I, [V, V]),
+        "rh3t_instance_times": (I, [V, V, V, V]),
+        "rh3t_instance_status": (I, [V, V]),
+        "rh3t_set_tile_shapes": (I, [V, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
+        "rh3t_get_tile_shapes": (I, [V, C.c_int32, V]),
+        "rh3t_autotune": (I, [V, C.c_char_p, C.c_int32, V, C.c_int32, P(C.c_int32)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

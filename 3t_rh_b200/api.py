@@ -23,10 +23,18 @@ OUTER, INNER = 0, 1
 class RH3TError(RuntimeError):
     """A failure the reference reports with panic! (main.rs:30-33, ghost.rs:229-263, bc1.rs:467-469, ...)."""
 
-    def __init__(self, code, message, stage=0, step=0, i=0, j=0, ghost=-1):
+    def __init__(self, code, message, stage=0, step=0, i=0, j=0, ghost=-1, instance=-1):
         self.code, self.stage, self.step, self.i, self.j, self.ghost = code, stage, step, i, j, ghost
+        self.instance = instance
         self.kind = _lib.STATUS_NAMES.get(code, str(code))
-        super().__init__(f"{message} [{self.kind}; step {step}, stage {stage}, idx ({i}, {j}), ghost {ghost}]")
+        where = f", instance {instance}" if instance > 0 else ""
+        super().__init__(f"{message} [{self.kind}; step {step}, stage {stage}, idx ({i}, {j}), ghost {ghost}{where}]")
+
+
+def _raise_last(L, h, rc):
+    e = _lib.Error()
+    L.rh3t_last_error(h, C.byref(e))
+    raise RH3TError(e.code or rc, e.message.decode(), e.stage, e.step, e.i, e.j, e.ghost, e.instance)
 
 
 def _arr(a, dtype):
@@ -366,9 +374,7 @@ class Solver:
 
     def _check(self, rc):
         if rc:
-            e = _lib.Error()
-            self.L.rh3t_last_error(self.h, C.byref(e))
-            raise RH3TError(e.code or rc, e.message.decode(), e.stage, e.step, e.i, e.j, e.ghost)
+            _raise_last(self.L, self.h, rc)
 
     def close(self):
         if getattr(self, "h", None):
@@ -427,6 +433,150 @@ class Solver:
         d = C.c_double()
         self._check(self.L.rh3t_last_dt(self.h, C.byref(d)))
         return d.value
+
+    def synchronize(self):
+        self._check(self.L.rh3t_synchronize(self.h))
+
+    @property
+    def kernel_launches(self):
+        return int(self.L.rh3t_kernel_launches(self.h))
+
+    @property
+    def stream(self):
+        return self.L.rh3t_stream(self.h)
+
+
+class Batch:
+    """Independent instances (Field + GhostGrid each, any sizes, parameters
+    and BCs) resident together on one GPU (rh3t_batch_create). Every kernel
+    launch covers all instances; each instance has its own dt reduction, time
+    and error record, and advance() replays one CUDA graph per step of the
+    whole batch. No reference counterpart: the reference runs one Field per
+    process."""
+
+    def __init__(self, fields, ghostgrids, device=0, exact=False):
+        if len(fields) != len(ghostgrids) or not fields:
+            raise ValueError("one GhostGrid per Field, at least one")
+        self.L = _lib.load(exact)
+        self.exact = exact
+        self.n = len(fields)
+        self.grids = [f.grid for f in fields]
+        self.n_ghosts = [g.len() for g in ghostgrids]
+        self.cells = np.array([f.grid.len() for f in fields], np.int64)
+        self.offsets = np.concatenate([[0], np.cumsum(self.cells)])
+        keep = []  # the C views must outlive rh3t_batch_create
+        desc = (_lib.Instance * self.n)()
+        for k, (f, g) in enumerate(zip(fields, ghostgrids)):
+            grid, prm = f.grid.to_c(), f.params.to_c()
+            obc = (_lib.BC * max(1, len(f.bc_outer)))(*[b.to_c() for b in f.bc_outer])
+            ibc = (_lib.BC * max(1, len(f.bc_inner)))(*[b.to_c() for b in f.bc_inner])
+            fluid = _arr(f.fluid, np.uint8)
+            table = g.to_c()
+            keep += [grid, prm, obc, ibc, fluid, table]
+            desc[k] = _lib.Instance(C.addressof(grid), C.addressof(prm), fluid.ctypes.data, len(f.bc_outer),
+                                    C.addressof(obc), len(f.bc_inner), C.addressof(ibc), C.addressof(table))
+        h = C.c_void_p()
+        rc = self.L.rh3t_batch_create(self.n, C.addressof(desc), device, C.byref(h))
+        if rc:
+            raise RH3TError(rc, "rh3t_batch_create failed")
+        self.h = h
+        self.upload(fields)
+
+    def _check(self, rc):
+        if rc:
+            _raise_last(self.L, self.h, rc)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.rh3t_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def upload(self, fields):
+        v = np.concatenate([_arr(f.value, np.float64).reshape(-1) for f in fields])
+        t = np.array([f.time for f in fields], np.float64)
+        self._check(self.L.rh3t_upload_batch(self.h, v.ctypes.data, t.ctypes.data))
+
+    def upload_values(self, values, times):
+        """values: all instances' value arrays concatenated (total_cells x 6)."""
+        v = _arr(values, np.float64)
+        t = _arr(times, np.float64)
+        self._check(self.L.rh3t_upload_batch(self.h, v.ctypes.data, t.ctypes.data))
+
+    def download_values(self):
+        """(total_cells x 6 values of all instances, times[n])"""
+        out = np.zeros((int(self.offsets[-1]), 6))
+        t = np.zeros(self.n)
+        self._check(self.L.rh3t_download_batch(self.h, out.ctypes.data, t.ctypes.data))
+        return out, t
+
+    def download(self, k=None):
+        """[(value, time)] per instance, or one instance's (value, time)."""
+        if k is not None:
+            out = np.zeros((int(self.cells[k]), 6))
+            t = C.c_double()
+            self._check(self.L.rh3t_download_instance(self.h, int(k), out.ctypes.data, C.byref(t)))
+            return out, t.value
+        v, t = self.download_values()
+        return [(v[self.offsets[k]:self.offsets[k + 1]], float(t[k])) for k in range(self.n)]
+
+    def l(self, k, with_ghosts=False):
+        rhs = np.zeros((int(self.cells[k]), 6))
+        gv = np.zeros((self.n_ghosts[k], 6)) if with_ghosts else None
+        self._check(self.L.rh3t_l_instance(self.h, int(k), rhs.ctypes.data, _ptr(gv)))
+        return (rhs, gv) if with_ghosts else rhs
+
+    def calc_global_dt(self):
+        d = np.zeros(self.n)
+        self._check(self.L.rh3t_calc_global_dt_batch(self.h, d.ctypes.data))
+        return d
+
+    def rk3_ssp(self, dt):
+        self._check(self.L.rh3t_rk3_ssp(self.h, float(dt)))
+
+    def advance(self, nsteps, cfl_factor=0.05, t_final=math.inf, graph=True):
+        self._check(self.L.rh3t_advance(self.h, int(nsteps), float(cfl_factor), float(t_final), int(bool(graph))))
+
+    def times(self):
+        """(time, dt of the last step, steps taken) per instance"""
+        t, dt, n = np.zeros(self.n), np.zeros(self.n), np.zeros(self.n, np.int64)
+        self._check(self.L.rh3t_instance_times(self.h, t.ctypes.data, dt.ctypes.data, n.ctypes.data))
+        return t, dt, n
+
+    def status(self):
+        """per-instance status codes of the last synchronising call"""
+        c = np.zeros(self.n, np.int32)
+        self._check(self.L.rh3t_instance_status(self.h, c.ctypes.data))
+        return c
+
+    def set_tile_shapes(self, lg_fx, lg_fy, lg_rhs, k=-1):
+        self._check(self.L.rh3t_set_tile_shapes(self.h, int(k), int(lg_fx), int(lg_fy), int(lg_rhs)))
+
+    def tile_shapes(self, k):
+        a = np.zeros(3, np.int32)
+        self._check(self.L.rh3t_get_tile_shapes(self.h, int(k), a.ctypes.data))
+        return tuple(int(x) for x in a)
+
+    def autotune(self, cache_path=None, reps=5):
+        """Time every admissible tile shape per (nx, ny, diffusion) class and
+        apply the fastest; returns one dict per class."""
+        out = (_lib.TuneEntry * 64)()
+        n = C.c_int32()
+        path = cache_path.encode() if cache_path else None
+        self._check(self.L.rh3t_autotune(self.h, path, int(reps), C.addressof(out), 64, C.byref(n)))
+        res = []
+        for e in out[:n.value]:
+            res.append(dict(nx=e.nx, ny=e.ny, diffusion=e.diffusion, n_instances=e.n_instances,
+                            shape=(e.lg_fx, e.lg_fy, e.lg_rhs), from_cache=bool(e.from_cache),
+                            ms_fx=list(e.ms_fx), ms_fy=list(e.ms_fy), ms_rhs=list(e.ms_rhs)))
+        return res
+
+    def profile_steps(self, nsteps, cfl_factor=0.05):
+        ms = np.zeros(4)
+        cnt = np.zeros(4, np.int64)
+        self._check(self.L.rh3t_profile_steps(self.h, int(nsteps), float(cfl_factor), ms.ctypes.data, cnt.ctypes.data))
+        return dict(zip(("ghosts", "flux", "rhs_stage", "dt"), zip(ms.tolist(), cnt.tolist())))
 
     def synchronize(self):
         self._check(self.L.rh3t_synchronize(self.h))

@@ -6,6 +6,9 @@ keeps in init.rs, restated for inputs of the solver).
   init_double_mach  init.rs:26-113 (reference mesh width 1/320)
   planar_shock      translating Mach-2 shock, y-periodic (no reference builder)
   rect_field        bc1.rs:1641-1702 test fixture (one BC kind on all sides)
+  batch_specs       seeded half-cylinder instances of uneven size and
+                    parameters for the batched solver (the LCG of the
+                    reference's parity tests, main.rs:493-498)
 """
 import math
 
@@ -149,3 +152,46 @@ def rect_field(nx, ny, lx, ly, value, kind=BCType.WALL, params=None):
 
 def _round(v):
     return math.floor(v + 0.5) if v >= 0 else -math.floor(-v + 0.5)
+
+
+# ------------------------------------------------------------------ batched workloads
+BATCH_SEED = 20261203
+BATCH_SIZES = (61, 91, 121)
+OMEGA_BASE = 1.0  # the reference's exchange coefficients are 0 (constant.rs); the scaled base is 1
+
+
+class Lcg:
+    """main.rs:493-498: 64-bit LCG, uniform doubles in [0, 1) from the top 53 bits."""
+
+    MASK = (1 << 64) - 1
+
+    def __init__(self, seed):
+        self.state = int(seed) & self.MASK
+
+    def uniform(self):
+        self.state = (self.state * 6364136223846793005 + 1442695040888963407) & self.MASK
+        return float(self.state >> 11) / float(1 << 53)
+
+
+def batch_specs(n=256, seed=BATCH_SEED, sizes=BATCH_SIZES, mach=(2.0, 4.0), omega_scale=(0.1, 10.0),
+                omega_base=OMEGA_BASE):
+    """n half-cylinder instances: nx uniform over `sizes` (ny = 4 (nx - 1) + 1,
+    square cells h = 3 / (nx - 1)), inflow Mach uniform in `mach`, electron-ion
+    and electron-radiation exchange coefficients log-uniform in `omega_scale`
+    times `omega_base`. Draw order per instance: size, Mach, omega_ei, omega_er."""
+    rng = Lcg(seed)
+    lo, hi = math.log(omega_scale[0]), math.log(omega_scale[1])
+    out = []
+    for _ in range(n):
+        nx = sizes[min(int(rng.uniform() * len(sizes)), len(sizes) - 1)]
+        m = mach[0] + (mach[1] - mach[0]) * rng.uniform()
+        oei = omega_base * math.exp(lo + (hi - lo) * rng.uniform())
+        oer = omega_base * math.exp(lo + (hi - lo) * rng.uniform())
+        out.append(dict(nx=nx, ny=4 * (nx - 1) + 1, h=3.0 / (nx - 1), mach=m, omega_ei=oei, omega_er=oer))
+    return out
+
+
+def batch_field(spec):
+    """The half-cylinder Field of one batch_specs entry."""
+    return init_cylinder(h=spec["h"], mach=spec["mach"],
+                         params=Params(omega_ei=spec["omega_ei"], omega_er=spec["omega_er"]))

@@ -1,10 +1,11 @@
 // Interface fluxes (main.rs:165-246: weno.rs:685-802 reconstruction_fast per
 // x and y face, plus diffusion.rs:27-50 when diffusion is on).
 //
-// A block of 6 warps covers 64 faces in three phases:
-//   1. staging: the tile's stencil points (x tiles 8x8 faces -> 13x8 points,
-//      y tiles 64 faces -> 69 points) with their physical flux go to shared
-//      memory once (the reference evaluates them once per face, six times per
+// A block of 6 warps covers 64 faces (a TI x TJ tile, shape chosen per tile)
+// in three phases:
+//   1. staging: the tile's stencil points (x faces: (TI + 5) x TJ points,
+//      y faces: TI x (TJ + 5)) with their physical flux go to shared memory
+//      once (the reference evaluates them once per face, six times per
 //      point), and each face's Roe state and activity flag are formed once;
 //   2. characteristic pass: warp c owns characteristic field c for the 64
 //      faces (two per lane), so the row of L, the projections and the two
@@ -46,10 +47,14 @@ struct FluxShared {
     int act[FLUX_FACES];
 };
 
+// face f of the tile -> face (i, j), first stencil point p0 and point stride
 template <int DIR>
 __device__ __forceinline__ void face_index(const Tile& t, int f, int& i, int& j, int& p0, int& ps) {
-    if (DIR == 0) { i = t.i + f / FX_TJ; j = t.j0 + f % FX_TJ; p0 = f; ps = FX_TJ; }
-    else { i = t.i; j = t.j0 + f; p0 = f; ps = 1; }
+    const int r = f >> t.lg, cc = f & ((1 << t.lg) - 1);
+    i = t.i + r;
+    j = t.j0 + cc;
+    if (DIR == 0) { p0 = f; ps = 1 << t.lg; }
+    else { p0 = r * ((1 << t.lg) + 5) + cc; ps = 1; }
 }
 
 __device__ __forceinline__ void load_q(const FluxShared& S, int f, Roe& q, double& ics2, double& ib) {
@@ -125,15 +130,16 @@ __device__ __forceinline__ void flux_tile(const Inst& I, const Tile& t, int stag
     const double* __restrict__ buf = stage_src(I, stage);
     const long long plane = I.plane;
     const int nx = I.nx, ny = I.ny;
-    const int np = DIR == 0 ? (FX_TI + 5) * FX_TJ : FY_TJ + 5;
+    const int cols = 1 << t.lg, rows = FLUX_FACES >> t.lg;
+    const int np = DIR == 0 ? (rows + 5) * cols : rows * (cols + 5);
     const bool diff = I.diffusion != 0;
     // ---- 1. staging
     for (int w = threadIdx.x; w < np + FLUX_FACES; w += blockDim.x) {
         if (w < np) {
             const int p = w;
             int pi, pj;
-            if (DIR == 0) { pi = t.i - 3 + p / FX_TJ; pj = t.j0 + p % FX_TJ; }
-            else { pi = t.i; pj = t.j0 - 3 + p; }
+            if (DIR == 0) { pi = t.i - 3 + (p >> t.lg); pj = t.j0 + (p & (cols - 1)); }
+            else { const int r = p / (cols + 5); pi = t.i + r; pj = t.j0 - 3 + (p - r * (cols + 5)); }
             double s[6] = {1.0, 0.0, 0.0, 1.0, 1.0, 1.0};
             if (pi >= -RH3T_PAD && pi < nx + RH3T_PAD && pj >= -RH3T_PAD && pj < ny + RH3T_PAD)
                 load6(buf, plane, node_of(I, pi, pj), s);
@@ -154,7 +160,7 @@ __device__ __forceinline__ void flux_tile(const Inst& I, const Tile& t, int stag
             const int f = w - np;
             int i, j, p0, ps;
             face_index<DIR>(t, f, i, j, p0, ps);
-            bool valid = DIR == 0 ? (i <= nx && j < ny) : (j <= ny);
+            bool valid = DIR == 0 ? (i <= nx && j < ny) : (i < nx && j <= ny);
             if (valid) {
                 const uint8_t m0 = I.mask[node_of(I, i, j)];
                 const uint8_t m1 = DIR == 0 ? I.mask[node_of(I, i - 1, j)] : I.mask[node_of(I, i, j - 1)];

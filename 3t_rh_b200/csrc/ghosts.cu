@@ -1,0 +1,509 @@
+// Ghost-node update of one RK stage (ghost.rs:199-268 update_values_parallel,
+// bc1.rs:609-928 set_ghost_point_value with precomputed GhostBC data), in
+// two launches.
+//
+// k_ghost_prep, one thread per ghost:
+//   - heavy ghosts (Wall / Outflow / FarField): L, R and lambda at the
+//     nearest fluid node, rotated to the (normal, tangential) frame
+//     (bc1.rs:294-312), written into the ghost's record. Every thread runs
+//     the same six rows, so no lane waits on another's branch;
+//   - cheap ghosts (ReflectiveWall, ZerothOrder, Periodic, Constant,
+//     TimeDependent), six threads each, complete.
+// k_ghosts, heavy ghosts on persistent warps, one ghost at a time per warp.
+// A ghost's record (S_r, w, d, the E_r stencil and this stage's L, R,
+// lambda; 10.5 KB) arrives in shared memory by one bulk copy (cp.async.bulk,
+// completion on an mbarrier) issued one ghost ahead, so the table stream
+// overlaps the arithmetic. Per ghost:
+//   2. lanes spread over the 55 stencil nodes of E_0..E_4 (gathered before
+//      the record is awaited): rotate the momentum and project on the six
+//      characteristic fields (bc1.rs:209-219);
+//   3. lanes spread over the 55 rows of S_0..S_4: (S_r d_c)_a for all six c,
+//      summed over b in order (bc1.rs:224-229); S_r is stored transposed so
+//      the lanes of one order read consecutive words;
+//   4. lanes (c, r): beta_{c,r} = sum_a d_a (S d)_a and
+//      alpha = d_r / (eps + beta)^q; then a fixed balanced list of
+//      V^(k)_{c,r} = w_{r,k} . d per lane (bc1.rs:221-244);
+//   5. lanes (k, c): V^(k)_c = sum_r alpha_r / sum(alpha) V_r (bc1.rs:247-252);
+//   6. FarField rows, R products and the Taylor sum on lanes (bc1.rs:829-923);
+//      Wall (two 6x6 LU solves) and Outflow (LODI) on lane 0 (bc1.rs:691-828).
+// The per-k loop of the reference (bc1.rs:673-675) recomputes steps 2-4
+// unchanged; they are done once. Every sum keeps the reference's order, so
+// the no-contraction build reproduces the reference's values.
+#include <algorithm>
+
+#include "common.cuh"
+#include "kernels.cuh"
+#include "physics.cuh"
+
+namespace rh3t {
+
+constexpr int GH_WARPS = 4;
+constexpr int GH_BLOCKS_PER_SM = 2;
+constexpr int GH_PREP_THREADS = 128;
+constexpr int GH_WAIT_LIMIT = 1 << 20; // try_wait rounds before a wait counts as timed out
+constexpr int GH_TIMEOUT_CODE = 11;    // RH3T_ERR_DEVICE_TIMEOUT
+__constant__ int kStOff[6] = {0, 1, 5, 14, 30, 55};
+__constant__ int kSOff[6] = {0, 1, 17, 98, 354, 979};
+__constant__ int kWOff[6] = {0, 1, 9, 36, 100, 225};
+
+// Step 4 V work lists, one row per lane: (c << 6) | (r << 3) | k, k <= r;
+// 0xffff ends a list. Longest first (LPT) over the 90 dot products of
+// lengths (r+1)^2: 45 terms at most per lane for 1350 in total.
+constexpr int GH_VITEMS = 4;
+__constant__ unsigned short kVItems[32][GH_VITEMS] = {
+    {0x0020, 0x0058, 0x0108, 0xffff},
+    {0x0021, 0x0059, 0x0109, 0xffff},
+    {0x0022, 0x005a, 0x0148, 0xffff},
+    {0x0023, 0x005b, 0x0149, 0xffff},
+    {0x0024, 0x0098, 0x0000, 0xffff},
+    {0x0060, 0x0099, 0x0040, 0xffff},
+    {0x0061, 0x009a, 0x0080, 0xffff},
+    {0x0062, 0x009b, 0x00c0, 0xffff},
+    {0x0063, 0x00d8, 0x0100, 0xffff},
+    {0x0064, 0x00d9, 0x0140, 0xffff},
+    {0x00a0, 0x00da, 0xffff, 0xffff},
+    {0x00a1, 0x00db, 0xffff, 0xffff},
+    {0x00a2, 0x0118, 0xffff, 0xffff},
+    {0x00a3, 0x0119, 0xffff, 0xffff},
+    {0x00a4, 0x011a, 0xffff, 0xffff},
+    {0x00e0, 0x011b, 0xffff, 0xffff},
+    {0x00e1, 0x0158, 0xffff, 0xffff},
+    {0x00e2, 0x0159, 0xffff, 0xffff},
+    {0x00e3, 0x015a, 0xffff, 0xffff},
+    {0x00e4, 0x015b, 0xffff, 0xffff},
+    {0x0120, 0x0010, 0x0110, 0xffff},
+    {0x0121, 0x0011, 0x0111, 0xffff},
+    {0x0122, 0x0012, 0x0112, 0xffff},
+    {0x0123, 0x0050, 0x0150, 0xffff},
+    {0x0124, 0x0051, 0x0151, 0xffff},
+    {0x0160, 0x0052, 0x0152, 0xffff},
+    {0x0161, 0x0090, 0x0008, 0x0088},
+    {0x0162, 0x0091, 0x0009, 0x0089},
+    {0x0163, 0x0092, 0x0048, 0x00c8},
+    {0x0164, 0x00d0, 0x0049, 0x00c9},
+    {0x0018, 0x001a, 0x00d1, 0xffff},
+    {0x0019, 0x001b, 0x00d2, 0xffff},
+};
+
+struct GhostWarp {
+    double rec[2][GH_REC]; // double-buffered heavy records
+    double D[6][56];       // characteristic data d_c at stencil node a
+    double ACC[6][56];     // (S_r d_c) at stencil row a; later u[5][6] and vinf[6]
+    double alpha[6][5];
+    double V[6][15];       // [c][r (r + 1) / 2 + k], k <= r
+    double v[5][6];        // V^(k)_c
+    unsigned long long bar[2];
+};
+static_assert(sizeof(GhostWarp) % 16 == 0, "records stay 16-byte aligned");
+constexpr int GH_SMEM = GH_WARPS * (int)sizeof(GhostWarp);
+
+// ---------------------------------------------------------------- bulk copy
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_fence_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// one thread: expect `bytes` on bar, then copy global -> shared (16-byte
+// aligned addresses, bytes a multiple of 16)
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, unsigned long long* bar) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+// bounded wait for the phase with parity `parity` of bar
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, uint32_t parity) {
+    const uint32_t a = smem_u32(bar);
+    for (int it = 0; it < GH_WAIT_LIMIT; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ int row_order(int R) {
+    return R < 1 ? 0 : (R < 5 ? 1 : (R < 14 ? 2 : (R < 30 ? 3 : 4)));
+}
+
+// bc1.rs:467-469 solve6 with LAPACK getrf/getrs semantics
+__device__ bool solve6(double A[6][6], double b[6]) {
+    int piv[6];
+    for (int j = 0; j < 6; ++j) {
+        int p = j;
+        double mx = fabs(A[j][j]);
+        for (int i = j + 1; i < 6; ++i)
+            if (fabs(A[i][j]) > mx) { mx = fabs(A[i][j]); p = i; }
+        piv[j] = p;
+        if (A[p][j] == 0.0) return false;
+        if (p != j)
+            for (int k = 0; k < 6; ++k) { double t = A[j][k]; A[j][k] = A[p][k]; A[p][k] = t; }
+        double rcp = 1.0 / A[j][j];
+        for (int i = j + 1; i < 6; ++i) A[i][j] *= rcp;
+        for (int k = j + 1; k < 6; ++k)
+            for (int i = j + 1; i < 6; ++i) A[i][k] -= A[i][j] * A[j][k];
+    }
+    for (int j = 0; j < 6; ++j)
+        if (piv[j] != j) { double t = b[j]; b[j] = b[piv[j]]; b[piv[j]] = t; }
+    for (int k = 0; k < 6; ++k)
+        for (int i = k + 1; i < 6; ++i) b[i] -= b[k] * A[i][k];
+    for (int k = 5; k >= 0; --k) {
+        b[k] /= A[k][k];
+        for (int i = 0; i < k; ++i) b[i] -= b[k] * A[i][k];
+    }
+    return true;
+}
+
+// out[i] = sum_j R[i][j] x[j] with R stored by column (Rc[6 j + i])
+__device__ __forceinline__ void r_times(const double* Rc, const double x[6], double* out) {
+    for (int i = 0; i < 6; ++i) {
+        double acc = 0.0;
+        for (int j = 0; j < 6; ++j) acc += Rc[6 * j + i] * x[j];
+        out[i] = acc;
+    }
+}
+
+// Wall (bc1.rs:691-756) and Outflow (bc1.rs:760-828) rows on one lane;
+// fills u[5][6]. Returns false when an ILW system is singular.
+__device__ __noinline__ bool serial_tail(const Inst& I, const GhostRec& Rg, const double* __restrict__ rec,
+                                         const double (*v)[6], double (*u)[6]) {
+    const DevParams& P = I.P;
+    const double* L = rec + GH_L;
+    const double* Rc = rec + GH_R;
+    if (Rg.kind == BC_WALL) {
+        double A0[6][6], rhs0[6];
+        for (int i = 0; i < 6; ++i)
+            for (int k = 0; k < 6; ++k) A0[i][k] = L[6 * i + k];
+        for (int k = 0; k < 6; ++k) A0[0][k] = k == 1 ? 1.0 : 0.0;
+        for (int k = 0; k < 6; ++k) rhs0[k] = v[0][k];
+        rhs0[0] = 0.0;
+        if (!solve6(A0, rhs0)) return false;
+        for (int k = 0; k < 6; ++k) u[0][k] = rhs0[k];
+        const double gi = P.gamma_i - 1.0, ge = P.gamma_e - 1.0, gr = P.gamma_r - 1.0;
+        const double gt = gi + ge + gr;
+        const double u1 = u[0][0], u3 = u[0][2];
+        double row1[6] = {-gt * sqd(u3) / (6.0 * sqd(u1)), 0.0, gt * u3 / (6.0 * u1), -ge, -gi, -gr};
+        double A1[6][6], rhs1[6];
+        for (int i = 0; i < 6; ++i)
+            for (int k = 0; k < 6; ++k) A1[i][k] = L[6 * i + k];
+        for (int k = 0; k < 6; ++k) A1[0][k] = row1[k];
+        for (int k = 0; k < 6; ++k) rhs1[k] = v[1][k];
+        rhs1[0] = 0.0;
+        if (!solve6(A1, rhs1)) return false;
+        for (int k = 0; k < 6; ++k) u[1][k] = rhs1[k];
+        for (int k = 2; k <= 4; ++k) r_times(Rc, v[k], u[k]);
+        return true;
+    }
+    // Outflow
+    const DevBC& bc = I.bcs[Rg.bc];
+    r_times(Rc, v[0], u[0]);
+    const double rho0 = u[0][0];
+    const double un0 = u[0][1] / rho0, ut0 = u[0][2] / rho0;
+    const double w2 = un0 * un0 + ut0 * ut0;
+    const double ee1 = u[0][3] / rho0 - w2 / 6.0, ei1 = u[0][4] / rho0 - w2 / 6.0, er1 = u[0][5] / rho0 - w2 / 6.0;
+    const double ge = P.gamma_e - 1.0, gi = P.gamma_i - 1.0, gr = P.gamma_r - 1.0;
+    const double p0 = rho0 * (ge * ee1 + gi * ei1 + gr * er1);
+    const double a2 = P.gamma_e * ge * ee1 + P.gamma_i * gi * ei1 + P.gamma_r * gr * er1;
+    const double a = sqrt(a2);
+    const double lambda1 = un0 - a;
+    double rhs1[6];
+    for (int k = 0; k < 6; ++k) rhs1[k] = v[1][k];
+    if (lambda1 < 0.0) {
+        const double m_local = fabs(un0 / a);
+        const double l1 = bc.sigma * (1.0 - sqd(m_local)) * a / bc.l_domain * (p0 - bc.p_inf);
+        rhs1[0] = l1 / lambda1;
+    }
+    r_times(Rc, rhs1, u[1]);
+    for (int k = 2; k <= 4; ++k) r_times(Rc, v[k], u[k]);
+    return true;
+}
+
+// ---------------------------------------------------------------- preparation
+__device__ void cheap_ghost(const Inst& I, const GhostRec& Rg, int c, int stage) {
+    double* buf = const_cast<double*>(stage_src(I, stage));
+    const long long plane = I.plane;
+    const DevBC& bc = I.bcs[Rg.bc];
+    double val;
+    if (Rg.kind == BC_CONSTANT) {
+        val = bc.state[c]; // bc1.rs:631-633
+    } else if (Rg.kind == BC_TIME_DEPENDENT) {
+        const double xs = bc.td_x0 + bc.td_speed * I.sc->t_stage[stage]; // bc1.rs:634-636, init.rs:61-65
+        val = Rg.p0x <= xs ? bc.td_left[c] : bc.td_right[c];
+    } else if (Rg.kind == BC_REFLECTIVE_WALL) {
+        double s[6]; // bc1.rs:930-1037
+        load6(buf, plane, Rg.src, s);
+        const double mom_n = s[1] * Rg.nx + s[2] * Rg.ny;
+        val = c == 1 ? s[1] - 2.0 * mom_n * Rg.nx : (c == 2 ? s[2] - 2.0 * mom_n * Rg.ny : s[c]);
+    } else {
+        val = buf[c * plane + Rg.src]; // ZerothOrder bc1.rs:471-545, Periodic bc1.rs:547-607
+    }
+    if (!isfinite(val)) report(I, 1 + 2 * stage, 2, (unsigned)Rg.gid);
+    buf[c * plane + Rg.node] = val;
+}
+
+// blocks [0, nbp): L, R, lambda of one heavy ghost per thread; then cheap ghosts
+__global__ void __launch_bounds__(GH_PREP_THREADS) k_ghost_prep(const Inst* __restrict__ insts,
+                                                               const GhostRec* __restrict__ heavy, int nh,
+                                                               const GhostRec* __restrict__ cheap, int nc,
+                                                               double* __restrict__ hrec, int stage, int nbp) {
+    if ((int)blockIdx.x < nbp) {
+        const int g = blockIdx.x * GH_PREP_THREADS + threadIdx.x;
+        if (g >= nh) return;
+        const GhostRec Rg = heavy[g];
+        const Inst& I = insts[Rg.inst];
+        if (has_error(I)) return;
+        const DevParams& P = I.P;
+        double s[6];
+        load6(stage_src(I, stage), I.plane, Rg.src, s);
+        const double mom_n = s[1] * Rg.nx + s[2] * Rg.ny;
+        const double mom_t = -s[1] * Rg.ny + s[2] * Rg.nx;
+        const double q6[6] = {s[0], mom_n, mom_t, s[3], s[4], s[5]};
+        const Prim d1 = prim_from_state(q6, P);
+        const Roe q = roe_average(q6[0], d1, q6[0], d1, P);
+        double* r = hrec + (size_t)Rg.heavy * GH_REC;
+        for (int row = 0; row < 6; ++row) {
+            double Lr[6], Rc[6], lam;
+            l_row<0>(row, q, P, Lr);
+            r_col<0>(row, q, P, Rc, lam);
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+                r[GH_L + 6 * row + k] = Lr[k];
+                r[GH_R + 6 * row + k] = Rc[k];
+            }
+            r[GH_LAM + row] = lam;
+        }
+    } else {
+        const int t = (blockIdx.x - nbp) * GH_PREP_THREADS + threadIdx.x;
+        const int g = t / 6, c = t - 6 * (t / 6);
+        if (g >= nc) return;
+        const GhostRec Rg = cheap[g];
+        const Inst& I = insts[Rg.inst];
+        if (has_error(I)) return;
+        cheap_ghost(I, Rg, c, stage);
+    }
+}
+
+// ---------------------------------------------------------------- heavy ghosts
+// characteristic data of stencil node a from its state (bc1.rs:209-219)
+__device__ __forceinline__ void project_node(GhostWarp& G, const double* __restrict__ L, const double s[6],
+                                             double nx, double ny, int a) {
+    const double mn = s[1] * nx + s[2] * ny;
+    const double mt = -s[1] * ny + s[2] * nx;
+    const double u6[6] = {s[0], mn, mt, s[3], s[4], s[5]};
+#pragma unroll
+    for (int c = 0; c < 6; ++c)
+        G.D[c][a] = L[6 * c + 0] * u6[0] + L[6 * c + 1] * u6[1] + L[6 * c + 2] * u6[2] + L[6 * c + 3] * u6[3] +
+                    L[6 * c + 4] * u6[4] + L[6 * c + 5] * u6[5];
+}
+
+// row R of S_r d_c for all six c (S_r transposed in the record)
+__device__ __forceinline__ void acc_row(GhostWarp& G, const double* __restrict__ rec, int R) {
+    const int r = row_order(R);
+    const int m = (r + 1) * (r + 1), off = kStOff[r], a = R - off;
+    const double* __restrict__ St = rec + GH_S + kSOff[r] + a;
+    double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll 5
+    for (int b = 0; b < m; ++b) {
+        const double sv = St[b * m];
+#pragma unroll
+        for (int c = 0; c < 6; ++c) acc[c] += sv * G.D[c][off + b];
+    }
+#pragma unroll
+    for (int c = 0; c < 6; ++c) G.ACC[c][R] = acc[c];
+}
+
+__device__ void heavy_ghost(const Inst& I, const GhostRec& Rg, GhostWarp& G, const double* __restrict__ rec,
+                            int lane, int stage, int row1, int row2, const unsigned short vitems[GH_VITEMS],
+                            const double s0[6], const double s1[6]) {
+    const DevParams& P = I.P;
+    double* buf = const_cast<double*>(stage_src(I, stage));
+    const long long plane = I.plane;
+    const double nx = Rg.nx, ny = Rg.ny;
+    const double* __restrict__ L = rec + GH_L;
+    const double* __restrict__ Rc = rec + GH_R;
+    const double* __restrict__ lam = rec + GH_LAM;
+    // 2. characteristic data of the 55 stencil nodes
+    project_node(G, L, s0, nx, ny, lane);
+    if (lane + 32 < 55) project_node(G, L, s1, nx, ny, lane + 32);
+    __syncwarp();
+    // 3. rows of S_r d_c
+    acc_row(G, rec, row1);
+    if (row2 >= 0) acc_row(G, rec, row2);
+    __syncwarp();
+    // 4a. beta and alpha, lanes (c, r)
+    if (lane < 30) {
+        const int c = lane / 5, r = lane - 5 * (lane / 5);
+        const int m = (r + 1) * (r + 1), off = kStOff[r];
+        double beta = 0.0;
+        for (int a = 0; a < m; ++a) beta += G.D[c][off + a] * G.ACC[c][off + a];
+        G.alpha[c][r] = rec[GH_D + r] / pow_q(P.eps + beta, P.weno_q);
+    }
+    // 4b. V^(k)_{c,r} = w_{r,k} . d
+#pragma unroll
+    for (int q = 0; q < GH_VITEMS; ++q) {
+        const unsigned e = vitems[q];
+        if (e == 0xffffu) break;
+        const int c = (int)(e >> 6), r = (int)((e >> 3) & 7u), k = (int)(e & 7u);
+        const int m = (r + 1) * (r + 1), off = kStOff[r];
+        const double* __restrict__ w = rec + GH_W + kWOff[r] + k * m;
+        double v = 0.0;
+        for (int a = 0; a < m; ++a) v += w[a] * G.D[c][off + a];
+        G.V[c][r * (r + 1) / 2 + k] = v;
+    }
+    __syncwarp();
+    // 5. nonlinear weights (bc1.rs:247-252); V^(k)_r = 0 for k > r
+    if (lane < 30) {
+        const int k = lane / 6, c = lane - 6 * (lane / 6);
+        double asum = 0.0;
+        for (int r = 0; r < 5; ++r) asum += G.alpha[c][r];
+        double res = 0.0;
+        for (int r = 0; r < 5; ++r)
+            res += (G.alpha[c][r] / asum) * (k <= r ? G.V[c][r * (r + 1) / 2 + k] : 0.0);
+        G.v[k][c] = res;
+    }
+    __syncwarp();
+    // 6. BC rows, R products, Taylor expansion (bc1.rs:690-924)
+    double (*u)[6] = reinterpret_cast<double (*)[6]>(&G.ACC[0][0]); // ACC is dead here
+    double* vinf = &G.ACC[5][0];
+    bool ok = true;
+    if (Rg.kind == BC_FAR_FIELD) {
+        const DevBC& bc = I.bcs[Rg.bc];
+        if (lane < 6) {
+            const double* ui = bc.state;
+            const double uinf[6] = {ui[0], ui[1] * nx + ui[2] * ny, -ui[1] * ny + ui[2] * nx, ui[3], ui[4], ui[5]};
+            double acc = 0.0;
+            for (int j = 0; j < 6; ++j) acc += L[6 * lane + j] * uinf[j];
+            vinf[lane] = acc;
+        }
+        __syncwarp();
+        if (lane < 30) {
+            const int k = lane / 6, i = lane - 6 * (lane / 6);
+            double acc = 0.0;
+            for (int m2 = 0; m2 < 6; ++m2) {
+                const double x = lam[m2] < 0.0 ? (k == 0 ? vinf[m2] : 0.0) : G.v[k][m2];
+                acc += Rc[6 * m2 + i] * x;
+            }
+            u[k][i] = acc;
+        }
+    } else if (lane == 0) {
+        ok = serial_tail(I, Rg, rec, G.v, u);
+    }
+    __syncwarp();
+    ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+    if (!ok) {
+        if (lane == 0) report(I, 1 + 2 * stage, 3, (unsigned)Rg.gid);
+        return;
+    }
+    double g = 0.0;
+    if (lane < 6) {
+        g = u[0][lane];
+        double coef = 1.0;
+        for (int k = 1; k <= 4; ++k) {
+            coef *= Rg.dist / (double)k;
+            g = g + coef * u[k][lane];
+        }
+    }
+    const double mn = __shfl_sync(0xffffffffu, g, 1), mt = __shfl_sync(0xffffffffu, g, 2);
+    if (lane < 6) {
+        const double out = lane == 1 ? mn * nx - mt * ny : (lane == 2 ? mn * ny + mt * nx : g);
+        buf[lane * plane + Rg.node] = out;
+        if (!isfinite(out)) report(I, 1 + 2 * stage, 2, (unsigned)Rg.gid);
+    }
+}
+
+// stencil states of ghost g (lane a and a + 32), from the record in global memory
+__device__ __forceinline__ void gather_stencil(const Inst& I, const double* __restrict__ grec, int lane, int stage,
+                                               double s0[6], double s1[6]) {
+    const int32_t* st = reinterpret_cast<const int32_t*>(grec + GH_ST);
+    const double* buf = stage_src(I, stage);
+    load6(buf, I.plane, st[lane], s0);
+    if (lane + 32 < 55) load6(buf, I.plane, st[lane + 32], s1);
+}
+
+__global__ void __launch_bounds__(GH_WARPS * 32) k_ghosts(const Inst* __restrict__ insts,
+                                                         const GhostRec* __restrict__ heavy, int nh,
+                                                         const double* __restrict__ hrec, int stage) {
+    extern __shared__ __align__(128) unsigned char gh_smem[];
+    const int lane = threadIdx.x & 31;
+    GhostWarp& G = reinterpret_cast<GhostWarp*>(gh_smem)[threadIdx.x >> 5];
+    const int stride = gridDim.x * GH_WARPS;
+    int g = blockIdx.x * GH_WARPS + (threadIdx.x >> 5);
+    if (g >= nh) return; // warp-uniform
+    // per-lane schedules of steps 3 and 4
+    const int row1 = lane < 25 ? 30 + lane : 14 + (lane - 25);
+    const int row2 = lane < 2 ? 28 + lane
+                     : lane < 11 ? 5 + (lane - 2)
+                     : lane < 15 ? 1 + (lane - 11)
+                     : lane == 15 ? 0
+                     : lane >= 25 ? 21 + (lane - 25) : -1;
+    unsigned short vitems[GH_VITEMS];
+#pragma unroll
+    for (int q = 0; q < GH_VITEMS; ++q) vitems[q] = kVItems[lane][q];
+    if (lane == 0) {
+        mbar_init(&G.bar[0]);
+        mbar_init(&G.bar[1]);
+        mbar_fence_init();
+        bulk_load(G.rec[0], hrec + (size_t)heavy[g].heavy * GH_REC, GH_REC * 8, &G.bar[0]);
+    }
+    __syncwarp();
+    for (int it = 0; g < nh; ++it, g += stride) {
+        const int b = it & 1;
+        const int gn = g + stride;
+        if (lane == 0 && gn < nh)
+            bulk_load(G.rec[b ^ 1], hrec + (size_t)heavy[gn].heavy * GH_REC, GH_REC * 8, &G.bar[b ^ 1]);
+        const GhostRec Rg = heavy[g];
+        const Inst& I = insts[Rg.inst];
+        const bool skip = has_error(I);
+        double s0[6], s1[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        if (!skip) gather_stencil(I, hrec + (size_t)Rg.heavy * GH_REC, lane, stage, s0, s1);
+        const bool ok = __all_sync(0xffffffffu, mbar_wait(&G.bar[b], (uint32_t)((it >> 1) & 1)));
+        if (!ok) {
+            if (lane == 0) report(I, 1 + 2 * stage, GH_TIMEOUT_CODE, (unsigned)Rg.gid);
+            if (gn < nh) mbar_wait(&G.bar[b ^ 1], (uint32_t)(((it + 1) >> 1) & 1)); // drain the prefetch
+            return;
+        }
+        if (!skip) heavy_ghost(I, Rg, G, G.rec[b], lane, stage, row1, row2, vitems, s0, s1);
+        __syncwarp();
+    }
+}
+
+void launch_ghosts(cudaStream_t s, const Inst* insts, const GhostRec* heavy, int nh, const GhostRec* cheap, int nc,
+                   double* hrec, int stage) {
+    if (nh + nc <= 0) return;
+    static int sm_count[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64) dev = 0;
+    if (sm_count[dev] == 0) {
+        int n = 0;
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        cudaFuncSetAttribute(k_ghosts, cudaFuncAttributeMaxDynamicSharedMemorySize, GH_SMEM);
+        sm_count[dev] = n > 0 ? n : 1;
+    }
+    const int nbp = (nh + GH_PREP_THREADS - 1) / GH_PREP_THREADS;
+    const int nbc = (nc * 6 + GH_PREP_THREADS - 1) / GH_PREP_THREADS;
+    k_ghost_prep<<<nbp + nbc, GH_PREP_THREADS, 0, s>>>(insts, heavy, nh, cheap, nc, hrec, stage, nbp);
+    if (nh > 0) {
+        const int nbh = std::min((nh + GH_WARPS - 1) / GH_WARPS, GH_BLOCKS_PER_SM * sm_count[dev]);
+        k_ghosts<<<nbh, GH_WARPS * 32, GH_SMEM, s>>>(insts, heavy, nh, hrec, stage);
+    }
+}
+
+int ghost_launches(int nh, int nc) { return (nh + nc > 0 ? 1 : 0) + (nh > 0 ? 1 : 0); }
+
+} // namespace rh3t

@@ -1,286 +1,16 @@
-// rh3t device kernels (sm_100a, FP64). One launch of each kernel covers all
-// instances of a context or batch: cell and face kernels walk a list of
-// 128-wide tiles, the ghost kernel a list of ghost records, so the plain
-// solver is simply a batch of one.
+// rh3t device kernels (sm_100a, FP64): the dt reduction, layout transfers and
+// diagnostics. One launch of each kernel covers all instances of a context or
+// batch: cell and face kernels walk a list of tiles, the ghost kernel a list
+// of ghost records, so the plain solver is simply a batch of one.
 //
-// Per RK stage: k_ghosts (ghost.rs:199-268) -> k_flux (main.rs:165-246) ->
-// k_rhs_stage (main.rs:251-349). Per step: k_dt (main.rs:375-408, dt.rs)
-// first. dt, stage times and RK coefficients never leave the device.
+// Per step: k_dt (main.rs:375-408, dt.rs), then per RK stage k_ghosts
+// (ghosts.cu) -> k_flux (flux.cu) -> k_rhs_stage (rhs.cu). dt, stage times
+// and RK coefficients never leave the device.
 #include "common.cuh"
 #include "kernels.cuh"
 #include "physics.cuh"
 
 namespace rh3t {
-
-// ------------------------------------------------------------------ ghosts
-// 6 threads per ghost (threadIdx.x = characteristic component c), 32 ghosts
-// per block. Heavy ghosts (Wall / Outflow / FarField): thread c forms the c-th
-// characteristic data of the five E_r stencils, its smoothness indicators
-// beta_r = d^T S_r d and the V^(k) = w_{r,k} . d with the reference's
-// summation order (bc1.rs:193-255), once for all k (the reference repeats
-// this identical work for k = 0..4, bc1.rs:673-675). Thread 0 then applies
-// the BC rows, the Taylor expansion and the rotation (bc1.rs:690-924).
-struct GhostShared {
-    double L[6][6];
-    double R[6][6]; // R[col][row]
-    double lam[6];
-    double v[5][6];
-};
-
-__device__ __forceinline__ void matvec_cols(const double Rc[6][6], const double x[6], double out[6]) {
-    // out[i] = sum_j R[i][j] x[j], R stored by column: Rc[j][i]
-#pragma unroll
-    for (int i = 0; i < 6; ++i) {
-        double acc = 0.0;
-#pragma unroll
-        for (int j = 0; j < 6; ++j) acc += Rc[j][i] * x[j];
-        out[i] = acc;
-    }
-}
-
-__device__ __forceinline__ void matvec_rows(const double L[6][6], const double x[6], double out[6]) {
-#pragma unroll
-    for (int i = 0; i < 6; ++i) {
-        double acc = 0.0;
-#pragma unroll
-        for (int j = 0; j < 6; ++j) acc += L[i][j] * x[j];
-        out[i] = acc;
-    }
-}
-
-// bc1.rs:467-469 solve6 with LAPACK getrf/getrs semantics
-__device__ bool solve6(double A[6][6], double b[6]) {
-    int piv[6];
-    for (int j = 0; j < 6; ++j) {
-        int p = j;
-        double mx = fabs(A[j][j]);
-        for (int i = j + 1; i < 6; ++i)
-            if (fabs(A[i][j]) > mx) { mx = fabs(A[i][j]); p = i; }
-        piv[j] = p;
-        if (A[p][j] == 0.0) return false;
-        if (p != j)
-            for (int k = 0; k < 6; ++k) { double t = A[j][k]; A[j][k] = A[p][k]; A[p][k] = t; }
-        double rcp = 1.0 / A[j][j];
-        for (int i = j + 1; i < 6; ++i) A[i][j] *= rcp;
-        for (int k = j + 1; k < 6; ++k)
-            for (int i = j + 1; i < 6; ++i) A[i][k] -= A[i][j] * A[j][k];
-    }
-    for (int j = 0; j < 6; ++j)
-        if (piv[j] != j) { double t = b[j]; b[j] = b[piv[j]]; b[piv[j]] = t; }
-    for (int k = 0; k < 6; ++k)
-        for (int i = k + 1; i < 6; ++i) b[i] -= b[k] * A[i][k];
-    for (int k = 5; k >= 0; --k) {
-        b[k] /= A[k][k];
-        for (int i = 0; i < k; ++i) b[i] -= b[k] * A[i][k];
-    }
-    return true;
-}
-
-template <int R_>
-__device__ __forceinline__ void extrap_order(const double* __restrict__ buf, long long plane,
-                                             const int32_t* __restrict__ st, const double* __restrict__ S,
-                                             const double* __restrict__ W, const double Lc[6], double nx, double ny,
-                                             double& beta, double vk[5]) {
-    constexpr int m = (R_ + 1) * (R_ + 1);
-    double data[m];
-#pragma unroll
-    for (int a = 0; a < m; ++a) {
-        long long n = st[a];
-        double rho = buf[n], mx = buf[plane + n], my = buf[2 * plane + n];
-        double ee = buf[3 * plane + n], ei = buf[4 * plane + n], er = buf[5 * plane + n];
-        double mn = mx * nx + my * ny;
-        double mt = -mx * ny + my * nx;
-        data[a] = Lc[0] * rho + Lc[1] * mn + Lc[2] * mt + Lc[3] * ee + Lc[4] * ei + Lc[5] * er;
-    }
-    double b = 0.0;
-#pragma unroll
-    for (int a = 0; a < m; ++a) {
-        double acc = 0.0;
-#pragma unroll
-        for (int q = 0; q < m; ++q) acc += S[a * m + q] * data[q];
-        b += data[a] * acc;
-    }
-    beta = b;
-#pragma unroll
-    for (int k = 0; k < 5; ++k) {
-        double v = 0.0;
-        if (k <= R_) {
-#pragma unroll
-            for (int a = 0; a < m; ++a) v += W[k * m + a] * data[a];
-        }
-        vk[k] = v;
-    }
-}
-
-__global__ void __launch_bounds__(192) k_ghosts(const Inst* __restrict__ insts, const GhostRec* __restrict__ recs,
-                                                int n_recs, const int32_t* __restrict__ hv_st,
-                                                const double* __restrict__ hv_s, const double* __restrict__ hv_w,
-                                                const double* __restrict__ hv_d, int stage) {
-    __shared__ GhostShared sh[32];
-    const int c = threadIdx.x;
-    const int gl = threadIdx.y;
-    const int g = blockIdx.x * 32 + gl;
-    const bool active = g < n_recs;
-    GhostRec R;
-    const Inst* Ip = nullptr;
-    bool heavy = false;
-    const double* buf = nullptr;
-    long long plane = 0;
-    bool skip = true;
-    if (active) {
-        R = recs[g];
-        Ip = &insts[R.inst];
-        skip = has_error(*Ip);
-        buf = stage_src(*Ip, stage);
-        plane = Ip->plane;
-        heavy = R.heavy >= 0;
-    }
-    if (active && !skip && !heavy) {
-        const Inst& I = *Ip;
-        double val;
-        const DevBC& bc = I.bcs[R.bc];
-        if (R.kind == BC_CONSTANT) {
-            val = bc.state[c];
-        } else if (R.kind == BC_TIME_DEPENDENT) {
-            double xs = bc.td_x0 + bc.td_speed * I.sc->t_stage[stage];
-            val = R.p0x <= xs ? bc.td_left[c] : bc.td_right[c];
-        } else if (R.kind == BC_REFLECTIVE_WALL) {
-            double s[6];
-            load6(buf, plane, R.src, s);
-            double mom_n = s[1] * R.nx + s[2] * R.ny;
-            val = c == 1 ? s[1] - 2.0 * mom_n * R.nx : (c == 2 ? s[2] - 2.0 * mom_n * R.ny : s[c]);
-        } else { // ZerothOrder, Periodic: copy of the source node
-            val = buf[c * plane + R.src];
-        }
-        if (!isfinite(val)) report(I, 1 + 2 * stage, 2, (unsigned)R.gid);
-        const_cast<double*>(buf)[c * plane + R.node] = val;
-    }
-    if (active && !skip && heavy) {
-        const Inst& I = *Ip;
-        const DevParams& P = I.P;
-        double s[6];
-        load6(buf, plane, R.src, s);
-        // bc1.rs:294-312 build_local_plain: nearest state rotated to (n, t)
-        double mom_n = s[1] * R.nx + s[2] * R.ny;
-        double mom_t = -s[1] * R.ny + s[2] * R.nx;
-        double s1[6] = {s[0], mom_n, mom_t, s[3], s[4], s[5]};
-        Prim d1 = prim_from_state(s1, P);
-        Roe q = roe_average(s1[0], d1, s1[0], d1, P);
-        double Lc[6];
-        l_row<0>(c, q, P, Lc);
-        double Rc[6], lam;
-        r_col<0>(c, q, P, Rc, lam);
-#pragma unroll
-        for (int k = 0; k < 6; ++k) { sh[gl].L[c][k] = Lc[k]; sh[gl].R[c][k] = Rc[k]; }
-        sh[gl].lam[c] = lam;
-        const long long h = R.heavy;
-        const int32_t* st = hv_st + h * 55;
-        const double* S = hv_s + h * 979;
-        const double* W = hv_w + h * 225;
-        double beta[5], vk[5][5];
-        extrap_order<0>(buf, plane, st + 0, S + 0, W + 0, Lc, R.nx, R.ny, beta[0], vk[0]);
-        extrap_order<1>(buf, plane, st + 1, S + 1, W + 1, Lc, R.nx, R.ny, beta[1], vk[1]);
-        extrap_order<2>(buf, plane, st + 5, S + 17, W + 9, Lc, R.nx, R.ny, beta[2], vk[2]);
-        extrap_order<3>(buf, plane, st + 14, S + 98, W + 36, Lc, R.nx, R.ny, beta[3], vk[3]);
-        extrap_order<4>(buf, plane, st + 30, S + 354, W + 100, Lc, R.nx, R.ny, beta[4], vk[4]);
-        double alpha[5], asum = 0.0;
-#pragma unroll
-        for (int r = 0; r < 5; ++r) {
-            alpha[r] = hv_d[h * 5 + r] / pow_q(P.eps + beta[r], P.weno_q);
-            asum += alpha[r];
-        }
-#pragma unroll
-        for (int k = 0; k < 5; ++k) {
-            double res = 0.0;
-#pragma unroll
-            for (int r = 0; r < 5; ++r) res += (alpha[r] / asum) * vk[r][k];
-            sh[gl].v[k][c] = res;
-        }
-    }
-    __syncthreads();
-    if (!(active && !skip && heavy) || c != 0) return;
-    const Inst& I = *Ip;
-    const DevParams& P = I.P;
-    GhostShared& G = sh[gl];
-    double u[5][6];
-    if (R.kind == BC_WALL) {
-        // bc1.rs:691-756
-        double A0[6][6], rhs0[6];
-        for (int i = 0; i < 6; ++i)
-            for (int k = 0; k < 6; ++k) A0[i][k] = G.L[i][k];
-        for (int k = 0; k < 6; ++k) A0[0][k] = k == 1 ? 1.0 : 0.0;
-        for (int k = 0; k < 6; ++k) rhs0[k] = G.v[0][k];
-        rhs0[0] = 0.0;
-        if (!solve6(A0, rhs0)) { report(I, 1 + 2 * stage, 3, (unsigned)R.gid); return; }
-        for (int k = 0; k < 6; ++k) u[0][k] = rhs0[k];
-        const double gi = P.gamma_i - 1.0, ge = P.gamma_e - 1.0, gr = P.gamma_r - 1.0;
-        const double gt = gi + ge + gr;
-        double row1[6] = {-gt * sqd(u[0][2]) / (6.0 * sqd(u[0][0])), 0.0, gt * u[0][2] / (6.0 * u[0][0]), -ge, -gi,
-                          -gr};
-        double A1[6][6], rhs1[6];
-        for (int i = 0; i < 6; ++i)
-            for (int k = 0; k < 6; ++k) A1[i][k] = G.L[i][k];
-        for (int k = 0; k < 6; ++k) A1[0][k] = row1[k];
-        for (int k = 0; k < 6; ++k) rhs1[k] = G.v[1][k];
-        rhs1[0] = 0.0;
-        if (!solve6(A1, rhs1)) { report(I, 1 + 2 * stage, 3, (unsigned)R.gid); return; }
-        for (int k = 0; k < 6; ++k) u[1][k] = rhs1[k];
-        for (int k = 2; k <= 4; ++k) matvec_cols(G.R, G.v[k], u[k]);
-    } else if (R.kind == BC_OUTFLOW) {
-        // bc1.rs:760-828
-        const DevBC& bc = I.bcs[R.bc];
-        matvec_cols(G.R, G.v[0], u[0]);
-        double rho0 = u[0][0];
-        double un0 = u[0][1] / rho0, ut0 = u[0][2] / rho0;
-        double w2 = un0 * un0 + ut0 * ut0;
-        double ee1 = u[0][3] / rho0 - w2 / 6.0, ei1 = u[0][4] / rho0 - w2 / 6.0, er1 = u[0][5] / rho0 - w2 / 6.0;
-        double ge = P.gamma_e - 1.0, gi = P.gamma_i - 1.0, gr = P.gamma_r - 1.0;
-        double p0 = rho0 * (ge * ee1 + gi * ei1 + gr * er1);
-        double a2 = P.gamma_e * ge * ee1 + P.gamma_i * gi * ei1 + P.gamma_r * gr * er1;
-        double a = sqrt(a2);
-        double lambda1 = un0 - a;
-        double rhs1[6];
-        for (int k = 0; k < 6; ++k) rhs1[k] = G.v[1][k];
-        if (lambda1 < 0.0) {
-            double m_local = fabs(un0 / a);
-            double l1 = bc.sigma * (1.0 - sqd(m_local)) * a / bc.l_domain * (p0 - bc.p_inf);
-            rhs1[0] = l1 / lambda1;
-        }
-        matvec_cols(G.R, rhs1, u[1]);
-        for (int k = 2; k <= 4; ++k) matvec_cols(G.R, G.v[k], u[k]);
-    } else {
-        // FarField, bc1.rs:829-924
-        const DevBC& bc = I.bcs[R.bc];
-        const double* ui = bc.state;
-        double uinf[6] = {ui[0], ui[1] * R.nx + ui[2] * R.ny, -ui[1] * R.ny + ui[2] * R.nx, ui[3], ui[4], ui[5]};
-        double vinf[6];
-        matvec_rows(G.L, uinf, vinf);
-        double rk[6];
-        for (int k = 0; k < 6; ++k) rk[k] = G.lam[k] < 0.0 ? vinf[k] : G.v[0][k];
-        matvec_cols(G.R, rk, u[0]);
-        for (int kk = 1; kk <= 4; ++kk) {
-            for (int k = 0; k < 6; ++k) rk[k] = G.lam[k] < 0.0 ? 0.0 : G.v[kk][k];
-            matvec_cols(G.R, rk, u[kk]);
-        }
-    }
-    // Taylor expansion + rotation back (bc1.rs:733-755)
-    double gv[6];
-    for (int k = 0; k < 6; ++k) gv[k] = u[0][k];
-    double coef = 1.0;
-    for (int k = 1; k <= 4; ++k) {
-        coef *= R.dist / (double)k;
-        for (int cc = 0; cc < 6; ++cc) gv[cc] = gv[cc] + coef * u[k][cc];
-    }
-    double mn = gv[1], mt = gv[2];
-    double out[6] = {gv[0], mn * R.nx - mt * R.ny, mn * R.ny + mt * R.nx, gv[3], gv[4], gv[5]};
-    bool fin = true;
-    double* wbuf = const_cast<double*>(buf);
-    for (int k = 0; k < 6; ++k) {
-        fin = fin && isfinite(out[k]);
-        wbuf[k * plane + R.node] = out[k];
-    }
-    if (!fin) report(I, 1 + 2 * stage, 2, (unsigned)R.gid);
-}
 
 // ------------------------------------------------------------------ dt
 // Orderable 64-bit key of a double (total order, NaN excluded by the caller).
@@ -357,7 +87,8 @@ __global__ void __launch_bounds__(128) k_dt(const Inst* __restrict__ insts, cons
     }
 }
 
-// A step with a caller-given dt (rk3_ssp(dt), main.rs:351-373)
+// A step with a caller-given dt (rk3_ssp(dt), main.rs:351-373), instances
+// insts[0, n_inst)
 __global__ void k_set_dt(const Inst* __restrict__ insts, int n_inst, double dt) {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n_inst) return;
@@ -377,31 +108,45 @@ __global__ void k_set_dt(const Inst* __restrict__ insts, int n_inst, double dt) 
 }
 
 // ------------------------------------------------------------------ layout
-// AoS (i*ny+j, 6 doubles) <-> padded SoA planes of buffer U, fluid cells only.
-__global__ void k_scatter(const Inst* __restrict__ insts, int inst, const double* __restrict__ aos, double time) {
-    const Inst& I = insts[inst];
+// AoS (6 doubles per cell, i*ny+j, instance k at aos + 6*cell_off) <-> padded
+// SoA planes of buffer U, fluid cells only. blockIdx.y = instance - k0.
+__global__ void k_scatter(const Inst* __restrict__ insts, int k0, const double* __restrict__ aos,
+                          const double* __restrict__ times) {
+    const int k = k0 + blockIdx.y;
+    const Inst& I = insts[k];
     long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (l == 0) {
-        I.sc->t_after = time;
-        I.sc->t = time;
+        I.sc->t_after = times[k];
+        I.sc->t = times[k];
     }
     if (l >= (long long)I.nx * I.ny) return;
     int i = (int)(l / I.ny), j = (int)(l % I.ny);
     long long n = node_of(I, i, j);
     if (!I.mask[n]) return;
+    const double* a = aos + 6 * (I.cell_off + l);
 #pragma unroll
-    for (int c = 0; c < 6; ++c) I.U[c * I.plane + n] = aos[l * 6 + c];
+    for (int c = 0; c < 6; ++c) I.U[c * I.plane + n] = a[c];
 }
 
-__global__ void k_gather(const Inst* __restrict__ insts, int inst, double* __restrict__ aos) {
-    const Inst& I = insts[inst];
+__global__ void k_gather(const Inst* __restrict__ insts, int k0, double* __restrict__ aos) {
+    const Inst& I = insts[k0 + blockIdx.y];
     long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (l >= (long long)I.nx * I.ny) return;
     int i = (int)(l / I.ny), j = (int)(l % I.ny);
     long long n = node_of(I, i, j);
     bool f = I.mask[n] != 0;
+    double* a = aos + 6 * (I.cell_off + l);
 #pragma unroll
-    for (int c = 0; c < 6; ++c) aos[l * 6 + c] = f ? I.U[c * I.plane + n] : 0.0;
+    for (int c = 0; c < 6; ++c) a[c] = f ? I.U[c * I.plane + n] : 0.0;
+}
+
+// cfl_factor / t_final of instances [k0, k0 + n)
+__global__ void k_set_step(const Inst* __restrict__ insts, int k0, int n, double cfl, double t_final) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    DevScalars& sc = *insts[k0 + k].sc;
+    sc.cfl_factor = cfl;
+    sc.t_final = t_final;
 }
 
 // planes (6 x nx*ny) -> AoS, for rh3t_l's rhs
@@ -458,12 +203,6 @@ void launch_dfma(cudaStream_t s, int blocks, double* out, int iters) {
     k_dfma<<<blocks, 256, 0, s>>>(out, iters, 0.9999999, 1e-7);
 }
 
-void launch_ghosts(cudaStream_t s, const Inst* insts, const GhostRec* recs, int n, const int32_t* hst,
-                   const double* hs, const double* hw, const double* hd, int stage) {
-    if (n <= 0) return;
-    dim3 blk(6, 32);
-    k_ghosts<<<(n + 31) / 32, blk, 0, s>>>(insts, recs, n, hst, hs, hw, hd, stage);
-}
 void launch_dt(cudaStream_t s, const Inst* insts, const Tile* tc, int nt, int mode) {
     if (nt <= 0) return;
     k_dt<<<nt, 128, 0, s>>>(insts, tc, nt, mode);
@@ -471,11 +210,18 @@ void launch_dt(cudaStream_t s, const Inst* insts, const Tile* tc, int nt, int mo
 void launch_set_dt(cudaStream_t s, const Inst* insts, int n_inst, double dt) {
     k_set_dt<<<(n_inst + 127) / 128, 128, 0, s>>>(insts, n_inst, dt);
 }
-void launch_scatter(cudaStream_t s, const Inst* insts, int inst, long long ncell, const double* aos, double time) {
-    k_scatter<<<(unsigned)((ncell + 255) / 256), 256, 0, s>>>(insts, inst, aos, time);
+void launch_scatter(cudaStream_t s, const Inst* insts, int k0, int n, long long max_cells, const double* aos,
+                    const double* times) {
+    if (n <= 0) return;
+    k_scatter<<<dim3((unsigned)((max_cells + 255) / 256), (unsigned)n), 256, 0, s>>>(insts, k0, aos, times);
 }
-void launch_gather(cudaStream_t s, const Inst* insts, int inst, long long ncell, double* aos) {
-    k_gather<<<(unsigned)((ncell + 255) / 256), 256, 0, s>>>(insts, inst, aos);
+void launch_gather(cudaStream_t s, const Inst* insts, int k0, int n, long long max_cells, double* aos) {
+    if (n <= 0) return;
+    k_gather<<<dim3((unsigned)((max_cells + 255) / 256), (unsigned)n), 256, 0, s>>>(insts, k0, aos);
+}
+void launch_set_step(cudaStream_t s, const Inst* insts, int k0, int n, double cfl, double t_final) {
+    if (n <= 0) return;
+    k_set_step<<<(n + 127) / 128, 128, 0, s>>>(insts, k0, n, cfl, t_final);
 }
 void launch_planes_to_aos(cudaStream_t s, const double* planes, long long n, double* aos) {
     k_planes_to_aos<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(planes, n, aos);

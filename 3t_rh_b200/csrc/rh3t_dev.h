@@ -1,5 +1,7 @@
 // Device data layout of the rh3t solver (shared by host and device code).
 //
+// A context holds one or more independent instances (a batch); every kernel
+// launch covers a contiguous range of them through per-instance Inst records.
 // HBM layout of one solver instance:
 //   state buffers U, A, B: 6 component planes each, padded node grid
 //     (nx + 2*PAD) x nyp with nyp = round_up(ny + 2*PAD, 8); node (i, j)
@@ -83,6 +85,7 @@ struct DevError {
 struct Inst {
     int32_t nx, ny, nyp, n_tiles_dt;
     long long plane;                // (nx + 2*PAD) * nyp
+    long long cell_off;             // sum of nx*ny over the instances before this one
     double dx, dy;
     DevParams P;
     int32_t diffusion, source;
@@ -99,18 +102,38 @@ struct Inst {
     DevError* err;
 };
 
-// work tile. Cell tiles: 128 consecutive j at one i. x-face tiles: faces
-// i in [i, i+FX_TI) x j in [j0, j0+FX_TJ). y-face tiles: faces j in
-// [j0, j0+FY_TJ) at column i.
+// work tile. Cell (dt) tiles: CELL_TILE consecutive j at one i. Face and
+// RHS tiles: a (64 >> lg) x (1 << lg) block of x faces, y faces (64 faces,
+// i x j) or a (256 >> lg) x (1 << lg) block of cells (RHS), starting at
+// (i, j0). The shape is chosen per tile, so one launch can mix instances
+// tuned to different shapes.
 struct Tile {
-    int32_t inst, i, j0, pad_;
+    int32_t inst, i, j0, lg;
 };
 
+// Heavy-ghost record (one per GhostBC slot, bc1.rs:50-57), repacked at set-up
+// so one 16-byte-aligned bulk copy brings a ghost's data to shared memory:
+// S (979 doubles, offsets of bc1.rs:45-47, each S_r stored transposed) |
+// w (225) | d (5) | pad (1) | E_r stencil as 55 padded node indices (int32,
+// + 1 pad) | per stage: L (6x6, row-major), R (6x6, by column), lambda (6),
+// pad (2), written by the ghost preparation kernel.
+constexpr int GH_S = 0, GH_W = 979, GH_D = 1204, GH_ST = 1210;
+constexpr int GH_L = 1238, GH_R = 1274, GH_LAM = 1310;
+constexpr int GH_REC = 1318;                     // doubles per record (10544 bytes)
+
 constexpr int CELL_TILE = 128;
-constexpr int RHS_TI = 8, RHS_TJ = 32;           // RHS/stage tiles: RHS_TI x RHS_TJ cells
-constexpr int FX_TI = 8, FX_TJ = 8, FY_TJ = 64;
 constexpr int FLUX_FACES = 64;                   // faces per flux block
 constexpr int FLUX_THREADS = 192;                // 6 warps: one per characteristic field
-constexpr int FLUX_NPT = (FX_TI + 5) * FX_TJ;    // staged points per flux block (>= FY_TJ + 5)
+constexpr int RHS_THREADS = 256;                 // cells per RHS block
+// admissible shapes (log2 of the j extent)
+constexpr int FX_LG_MIN = 2, FX_LG_MAX = 4;      // x faces 16x4, 8x8, 4x16
+constexpr int FY_LG_MIN = 4, FY_LG_MAX = 6;      // y faces 4x16, 2x32, 1x64
+constexpr int RHS_LG_MIN = 4, RHS_LG_MAX = 6;    // cells 16x16, 8x32, 4x64
+constexpr int FX_LG_DEF = 3, FY_LG_DEF = 6, RHS_LG_DEF = 5;
+// staged points per flux block: max over shapes of (TI + 5) * TJ (x) and
+// TI * (TJ + 5) (y)
+constexpr int FLUX_NPT = 144;
+// RHS halo points: max over shapes of (TI + 8) * (TJ + 8)
+constexpr int RHS_NPT = 864;
 
 } // namespace rh3t

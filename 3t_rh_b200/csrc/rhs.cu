@@ -3,14 +3,14 @@
 // exchange source (source.rs:7-21) and the diffusion differences, then
 // u' = a u + b v + c dt rhs with the admissibility check (main.rs:22-33).
 //
-// A block covers RHS_TI x RHS_TJ cells. The pressures and the transport
+// A block covers TI x TJ = 256 cells (shape chosen per tile). The pressures and the transport
 // velocities of the nodes within reach of the 9-point non-conservative
 // stencils (the tile plus a 4-node halo, corners excluded) are computed once
 // into shared memory; the reference's access-table gathers (main.rs:276-277)
 // evaluate them once per use, 17 times per node.
 //
-// mode 0 writes the rhs (6 planes of nx*ny, i*ny+j) for l(); mode 1 applies
-// the stage update of `stage`.
+// mode 0 writes the rhs (6 planes of nx*ny, i*ny+j, instance k at
+// rhs_out + 6*cell_off) for l(); mode 1 applies the stage update of `stage`.
 #include "common.cuh"
 #include "kernels.cuh"
 #include "physics.cuh"
@@ -23,10 +23,7 @@ constexpr bool kExactR = true;
 constexpr bool kExactR = false;
 #endif
 
-constexpr int RHS_HI = RHS_TI + 8, RHS_HJ = RHS_TJ + 8;
-constexpr int RHS_NPT = RHS_HI * RHS_HJ;
-
-__global__ void __launch_bounds__(256) k_rhs_stage(const Inst* __restrict__ insts, const Tile* __restrict__ tiles,
+__global__ void __launch_bounds__(RHS_THREADS) k_rhs_stage(const Inst* __restrict__ insts, const Tile* __restrict__ tiles,
                                                    int nt, int stage, int mode, double* __restrict__ rhs_out) {
     __shared__ double sP[5][RHS_NPT]; // pe, pi, pr, u, v
     if (blockIdx.x >= nt) return;
@@ -37,10 +34,12 @@ __global__ void __launch_bounds__(256) k_rhs_stage(const Inst* __restrict__ inst
     const long long plane = I.plane;
     const double* __restrict__ src = stage_src(I, stage);
     const int nx = I.nx, ny = I.ny;
+    const int TJ = 1 << t.lg, TI = RHS_THREADS >> t.lg;
+    const int HJ = TJ + 8, NPT = (TI + 8) * HJ;
     // ---- stage node primitives (tile + 4-node cross halo)
-    for (int p = threadIdx.x; p < RHS_NPT; p += blockDim.x) {
-        const int hi = p / RHS_HJ, hj = p - hi * RHS_HJ;
-        const bool corner = (hi < 4 || hi >= RHS_TI + 4) && (hj < 4 || hj >= RHS_TJ + 4);
+    for (int p = threadIdx.x; p < NPT; p += blockDim.x) {
+        const int hi = p / HJ, hj = p - hi * HJ;
+        const bool corner = (hi < 4 || hi >= TI + 4) && (hj < 4 || hj >= TJ + 4);
         const int i = t.i - 4 + hi, j = t.j0 - 4 + hj;
         if (corner || i < -RH3T_PAD || i >= nx + RH3T_PAD || j < -RH3T_PAD || j >= ny + RH3T_PAD) continue;
         double s[6];
@@ -49,7 +48,7 @@ __global__ void __launch_bounds__(256) k_rhs_stage(const Inst* __restrict__ inst
         sP[0][p] = d.pe; sP[1][p] = d.pi; sP[2][p] = d.pr; sP[3][p] = d.u; sP[4][p] = d.v;
     }
     __syncthreads();
-    const int ti = threadIdx.x / RHS_TJ, tj = threadIdx.x - ti * RHS_TJ;
+    const int ti = threadIdx.x >> t.lg, tj = threadIdx.x & (TJ - 1);
     const int i = t.i + ti, j = t.j0 + tj;
     if (i >= nx || j >= ny) return;
     const long long n = node_of(I, i, j);
@@ -66,10 +65,10 @@ __global__ void __launch_bounds__(256) k_rhs_stage(const Inst* __restrict__ inst
         rhs[c] = -(fr - fl) * sx + -(ft - fb) * sy;
     }
     double pe[9], pi[9], pr[9], vel[9], ncx[3], ncy[3];
-    const int hc = (ti + 4) * RHS_HJ + (tj + 4);
+    const int hc = (ti + 4) * HJ + (tj + 4);
 #pragma unroll
     for (int q = 0; q < 9; ++q) {
-        const int p = hc + (q - 4) * RHS_HJ;
+        const int p = hc + (q - 4) * HJ;
         pe[q] = sP[0][p]; pi[q] = sP[1][p]; pr[q] = sP[2][p]; vel[q] = sP[3][p];
     }
     if (kExactR) noncon9(pe, pi, pr, vel, dx, ncx);
@@ -104,8 +103,9 @@ __global__ void __launch_bounds__(256) k_rhs_stage(const Inst* __restrict__ inst
     }
     if (mode == 0) {
         const long long ln = (long long)i * ny + j, lp = (long long)nx * ny;
+        double* __restrict__ ro = rhs_out + 6 * I.cell_off;
 #pragma unroll
-        for (int c = 0; c < 6; ++c) rhs_out[c * lp + ln] = rhs[c];
+        for (int c = 0; c < 6; ++c) ro[c * lp + ln] = rhs[c];
         return;
     }
     const DevScalars& sc = *I.sc;
@@ -142,7 +142,7 @@ __global__ void __launch_bounds__(256) k_rhs_stage(const Inst* __restrict__ inst
 
 void launch_rhs_stage(cudaStream_t s, const Inst* insts, const Tile* tc, int nt, int stage, int mode, double* rhs) {
     if (nt <= 0) return;
-    k_rhs_stage<<<nt, 256, 0, s>>>(insts, tc, nt, stage, mode, rhs);
+    k_rhs_stage<<<nt, RHS_THREADS, 0, s>>>(insts, tc, nt, stage, mode, rhs);
 }
 
 } // namespace rh3t

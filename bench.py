@@ -1,12 +1,17 @@
 """Benchmark of the rh3t B200 solver: cell-updates/s of the SSP-RK3 step.
 
 A step is one SSP-RK3 step (main.rs:459-466: dt = 0.05 * calc_global_dt, then
-rk3_ssp) of one solver instance; a cell-update is one fluid node advanced by
-one step. Default workload: the reference's Mach-3 half-cylinder refined to
-h = 1/320 (961 x 3841 nodes, 3,525,896 fluid cells), FP64.
+rk3_ssp) of every solver instance; a cell-update is one fluid node advanced by
+one step. Default workload (batch256): 256 independent half-cylinder
+instances of uneven size (nx in {61, 91, 121}, ny = 4 (nx - 1) + 1), inflow
+Mach number and exchange coefficients (seeded, cases.batch_specs), advanced
+together by the batched solver, each with its own dt; the line also carries
+the plain solver run one instance at a time on the same instances. The plain
+workloads are the reference's Mach-3 half-cylinder at h = 1/320 (cyl961,
+961 x 3841 nodes), 1/160 and 1/40, and the planar shock. FP64 throughout.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                  [--workload cyl961|cyl481|cyl121|planar] [--exact]
+                  [--workload batch256|cyl961|cyl481|cyl121|planar] [--exact]
 
 --impl reference times the reference algorithm's CPU implementation (the
 oracle restatement, OpenMP on all host cores; the Rust reference cannot be
@@ -34,6 +39,8 @@ WORKLOADS = {
     "cyl481": dict(kind="cylinder", h=1.0 / 160.0, name="half-cylinder Mach-3, 481x1921 nodes (h=1/160)"),
     "cyl121": dict(kind="cylinder", h=1.0 / 40.0, name="half-cylinder Mach-3, 121x481 nodes (h=1/40)"),
     "planar": dict(kind="planar", name="Mach-2 planar shock, 1024x8, y-periodic, diffusion+exchange on"),
+    "batch256": dict(kind="batch", n=256, name="256 half-cylinder instances, nx in {61,91,121}, ny = 4(nx-1)+1, "
+                     "Mach U[2,4], omega_ei/omega_er log-U[0.1,10] x 1.0, seed 20261203"),
 }
 PLANAR_PARAMS = dict(kappa_e=1e-3, kappa_i=1e-3, kappa_r=1e-3, omega_ei=1.0, omega_er=1.0, periodic_ly=0.03125)
 CFL = 0.05
@@ -55,6 +62,10 @@ def make_oracle(O, wl):
     if spec["kind"] == "cylinder":
         return O.Case.cylinder(h=spec["h"])
     return O.Case.planar_shock(**PLANAR_PARAMS)
+
+
+def oracle_batch_case(O, sp):
+    return O.Case.cylinder(h=sp["h"], mach=sp["mach"], omega_ei=sp["omega_ei"], omega_er=sp["omega_er"])
 
 
 class ClockSampler:
@@ -117,8 +128,37 @@ def replica_value(ms_local, cells_local, steps, dist=None, device="cpu"):
     return float(c.item()) * steps / (ms * 1e-3), ms
 
 
-def cpu_baseline(O, wl, budget_s=20.0):
+def batch_oracle_rate(O, specs, budget_s, max_steps=None):
+    """Oracle cell-updates/s over the batch instances taken in order, one step
+    each per round, until the time budget (or max_steps rounds) is spent."""
+    cases, cells = [], []
+    t_build = time.perf_counter()
+    for sp in specs:
+        cases.append(oracle_batch_case(O, sp))
+        cells.append(int(cases[-1].fluid().sum()))
+        if time.perf_counter() - t_build > budget_s:
+            break
+    build_s = time.perf_counter() - t_build
+    done, steps, el = 0, 0, 0.0
+    t0 = time.perf_counter()
+    while True:
+        for c, n in zip(cases, cells):
+            c.run(1, CFL)
+            done += n
+        steps += 1
+        el = time.perf_counter() - t0
+        if el > budget_s or (max_steps is not None and steps >= max_steps):
+            break
+    return done / el, len(cases), steps, el, build_s
+
+
+def cpu_baseline(O, wl, budget_s=20.0, specs=None):
     """The oracle (OpenMP, all host threads) on a bounded number of steps of the same workload."""
+    if specs is not None:
+        v, n_inst, steps, el, build_s = batch_oracle_rate(O, specs, budget_s)
+        return {"value": v, "unit": "cell-updates/s", "cores": O.max_threads(), "kind": "port",
+                "sample": f"{steps} SSP-RK3 step(s) of each of the first {n_inst} of the {len(specs)} instances, "
+                          f"{el:.1f} s, after a {build_s:.1f} s ghost-grid build"}
     t0 = time.perf_counter()
     case = make_oracle(O, wl)
     build_s = time.perf_counter() - t0
@@ -143,9 +183,24 @@ def run_reference(args):
     if rank != 0:
         return
     spec = WORKLOADS[args.workload]
+    threads = O.max_threads()
+    if spec["kind"] == "batch":
+        import importlib
+        rh = importlib.import_module("3t_rh_b200")
+        specs = rh.cases.batch_specs(spec["n"])
+        v, n_inst, steps, el, _ = batch_oracle_rate(O, specs, 60.0, max_steps=args.steps)
+        line = {"metric": "cell-updates/s", "value": v, "unit": "cell-updates/s", "n_gpus": args.gpus,
+                "steps": steps, "warmup": 0, "ms_per_step": 1e3 * el / steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+                "config": {"workload": spec["name"], "instances_timed": n_inst},
+                "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": threads, "kind": "port",
+                                 "sample": f"{steps} SSP-RK3 step(s) of each of the first {n_inst} instances "
+                                           f"(bounded at ~60 s of stepping)"},
+                "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
     case = make_oracle(O, args.workload)
     cells = int(case.fluid().sum())
-    threads = O.max_threads()
     for _ in range(min(args.warmup, 1)):
         case.run(1, CFL)
     # each timed step is one full SSP-RK3 step; the number of steps is capped so
@@ -169,13 +224,136 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_batch(args, rh, flops, torch, dist, world, rank, local):
+    """Batched workload: all instances in one Batch, one CUDA graph per step;
+    then the plain solver on the same instances one at a time."""
+    spec = WORKLOADS[args.workload]
+    specs = rh.cases.batch_specs(spec["n"])
+    t0 = time.perf_counter()
+    fields = [rh.cases.batch_field(sp) for sp in specs]
+    grids = [rh.GhostGrid.build(f) for f in fields]
+    build_s = time.perf_counter() - t0
+    b = rh.Batch(fields, grids, device=local, exact=args.exact)
+    cells = int(sum(int(f.fluid.sum()) for f in fields))
+    tune = b.autotune(reps=5)
+    step_fl, fl_launch = 0.0, 0.0
+    for f, g in zip(fields, grids):
+        nxf, nyf = flops.face_counts(f.fluid, f.grid.nx, f.grid.ny)
+        step_fl += flops.step_flops(int(f.fluid.sum()), nxf, nyf, g.len(), g.n_heavy(), False, True)
+        fl_launch += flops.flux_launch_flops(nxf, nyf, False)
+    stream = torch.cuda.ExternalStream(b.stream, device=torch.device(f"cuda:{local}"))
+    b.advance(args.warmup, CFL)
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = b.kernel_launches
+    ev0.record(stream)
+    b.advance(args.steps, CFL)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    launches = b.kernel_launches - l0
+    value, ms = replica_value(ms, cells, args.steps, dist, f"cuda:{local}")
+    sampler.stop()
+    clocks = sampler.summary()
+    prof = b.profile_steps(min(args.steps, 10), CFL)
+    flux_ms, flux_n = prof["flux"]
+    achieved = fl_launch / (flux_ms / flux_n * 1e-3) / 1e12
+    peak = rh.api.fp64_peak_tflops(local)
+    total_prof_ms = sum(v[0] for v in prof.values())
+
+    # the plain GPU path on the same instances, one instance at a time
+    k_plain = max(5, min(args.steps, 20))
+    plain_ms, plain_cells = 0.0, 0
+    for f, g in zip(fields, grids):
+        sv = rh.Solver(f, g, device=local, exact=args.exact)
+        sv.advance(3, CFL)
+        st = torch.cuda.ExternalStream(sv.stream, device=torch.device(f"cuda:{local}"))
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        sv.advance(k_plain, CFL)
+        e1.record(st)
+        torch.cuda.synchronize()
+        plain_ms += e0.elapsed_time(e1)
+        plain_cells += int(f.fluid.sum())
+        sv.close()
+    plain_value = plain_cells * k_plain / (plain_ms * 1e-3)
+
+    e2e = None
+    if not args.no_e2e:
+        vals, times = b.download_values()
+        host = torch.empty(vals.shape, dtype=torch.float64, pin_memory=True).numpy()
+        host[:] = vals
+        k_e2e = max(3, min(args.steps, 10))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(k_e2e):
+            b.upload_values(host, times)
+            b.advance(1, CFL)
+            v2, times = b.download_values()
+            host[:] = v2
+        el = time.perf_counter() - t0
+        nb = host.size * 8
+        e2e = {"value": world * cells * k_e2e / el, "unit": "cell-updates/s", "h2d_bytes_per_step": nb + 8 * b.n,
+               "d2h_bytes_per_step": nb + 8 * b.n,
+               "call": "rh3t_upload_batch + rh3t_advance(1 step) + rh3t_download_batch (all Field::value arrays)",
+               "steps": k_e2e}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        from oracle import oracle as O  # timed CPU baseline only
+        cpu = cpu_baseline(O, args.workload, specs=specs)
+
+    if rank == 0:
+        classes = {}
+        for sp in specs:
+            classes[sp["nx"]] = classes.get(sp["nx"], 0) + 1
+        line = {
+            "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": spec["name"], "instances": b.n, "instances_by_nx": classes,
+                       "scheme": "SSP-RK3, dt = 0.05 dt_cfl per step and instance", "fluid_cells": cells,
+                       "ghosts": int(sum(g.len() for g in grids)),
+                       "heavy_ghosts": int(sum(g.n_heavy() for g in grids)),
+                       "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "inputs larger than L2 (state buffers 3 x %.0f MB)" % (
+                           6 * 8 * sum((f.grid.nx + 8) * (f.grid.ny + 8) for f in fields) / 1e6),
+                       "arithmetic": "no FMA contraction" if args.exact else "FMA contraction",
+                       "ghost_build_s": round(build_s, 3),
+                       "tile_shapes": {f"{e['nx']}x{e['ny']}": e["shape"] for e in tune}},
+            "instances_per_s": value / cells * b.n,
+            "plain_one_at_a_time": {"value": plain_value, "unit": "cell-updates/s", "steps_per_instance": k_plain,
+                                    "batched_speedup": value / plain_value},
+            "roofline": {"bound": "fp64", "kernel": "k_flux (x+y interface WENO5 fluxes, all instances)",
+                         "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                         "traffic": FLUX_TRAFFIC_BYTES.get(args.workload) if not args.exact else None,
+                         "traffic_unit": "bytes per launch",
+                         "peak_source": "measured DFMA loop on this GPU (rh3t_fp64_peak)",
+                         "flops_per_launch": fl_launch, "launch_ms": flux_ms / flux_n,
+                         "kernel_share": {k: v[0] / total_prof_ms for k, v in prof.items()},
+                         "step_tflops": step_fl / (ms / args.steps * 1e-3) / 1e12, "step_flops": step_fl},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    b.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="cyl961", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="batch256", choices=sorted(WORKLOADS))
     ap.add_argument("--exact", action="store_true", help="bench the no-FMA-contraction build")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -203,6 +381,11 @@ def main():
                                 device_id=torch.device(f"cuda:{local}"))
 
     spec = WORKLOADS[args.workload]
+    if spec["kind"] == "batch":
+        run_batch(args, rh, flops, torch, dist, world, rank, local)
+        if dist:
+            dist.destroy_process_group()
+        return
     f = make_field(rh, args.workload)
     t0 = time.perf_counter()
     g = rh.GhostGrid.build(f)

@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define RH3T_ABI_VERSION 1
+#define RH3T_ABI_VERSION 2
 
 typedef enum {
     RH3T_OK = 0,
@@ -42,7 +42,8 @@ typedef enum {
     RH3T_ERR_INVALID_ARGUMENT = 7,
     RH3T_ERR_CUDA = 8,
     RH3T_ERR_NONPOSITIVE_DT = 9,    /* main.rs:464 assert!(dt > 0.0) */
-    RH3T_ERR_NO_DEVICE = 10
+    RH3T_ERR_NO_DEVICE = 10,
+    RH3T_ERR_DEVICE_TIMEOUT = 11    /* a bounded device-side wait ran out (no reference counterpart) */
 } rh3t_status;
 
 /* field1.rs:6-15 GridInfo: node-centred x = x0 + i*dx, y = y0 + j*dy */
@@ -123,6 +124,7 @@ typedef struct {
     int64_t step;     /* step of rh3t_advance in which it happened (0-based) */
     int32_t i, j;     /* cell index (code 1) or ghost grid index (code 2, 3, 4) */
     int32_t ghost;    /* ghost id (codes 2, 3, 4), else -1 */
+    int32_t instance; /* failing instance of a batch context (0 for a plain one), -1 if none */
     char message[160];
 } rh3t_error;
 
@@ -154,7 +156,14 @@ const char* rh3t_geom_last_error(const rh3t_geom* g);
 void rh3t_geom_destroy(rh3t_geom* g);
 
 /* ------------------------------------------------------------------ */
-/* Device solver, one instance                                         */
+/* Device solver                                                       */
+/* A context holds one instance (rh3t_create, the drop-in for the      */
+/* reference's single Field) or a batch of independent instances       */
+/* (rh3t_batch_create). Whole-context calls (rh3t_advance,             */
+/* rh3t_rk3_ssp, rh3t_profile_steps, rh3t_synchronize) act on every    */
+/* instance with one launch per kernel phase; the single-instance      */
+/* calls (rh3t_upload_state, rh3t_download_state, rh3t_l,              */
+/* rh3t_calc_global_dt, rh3t_last_dt) act on instance 0.               */
 /* ------------------------------------------------------------------ */
 typedef struct rh3t_ctx rh3t_ctx;
 
@@ -166,6 +175,66 @@ void rh3t_default_params(rh3t_params* out);
 int rh3t_create(const rh3t_grid* grid, const rh3t_params* params, const uint8_t* fluid,
                 int32_t n_outer_bc, const rh3t_bc* outer_bcs, int32_t n_inner_bc, const rh3t_bc* inner_bcs,
                 const rh3t_ghost_table* ghosts, int32_t device, rh3t_ctx** out);
+
+/* One instance of a batch: the arguments of rh3t_create. */
+typedef struct {
+    const rh3t_grid* grid;
+    const rh3t_params* params;
+    const uint8_t* fluid;
+    int32_t n_outer_bc;
+    const rh3t_bc* outer_bcs;
+    int32_t n_inner_bc;
+    const rh3t_bc* inner_bcs;
+    const rh3t_ghost_table* ghosts;
+} rh3t_instance;
+
+/* Batched solver (no reference counterpart: the reference advances one
+ * Field per process). n independent instances of any sizes, parameters and
+ * BCs, resident together; every kernel launch covers all of them, each
+ * instance keeps its own dt reduction, time and error record, and one step
+ * of the whole batch replays as one CUDA graph (rh3t_advance). */
+int rh3t_batch_create(int32_t n, const rh3t_instance* instances, int32_t device, rh3t_ctx** out);
+int32_t rh3t_instance_count(const rh3t_ctx* ctx);
+/* values: the instances' Field::value arrays concatenated in instance order;
+ * times: one Field::time per instance (may be NULL on download) */
+int rh3t_upload_batch(rh3t_ctx* ctx, const double* values, const double* times);
+int rh3t_download_batch(rh3t_ctx* ctx, double* values, double* times);
+int rh3t_upload_instance(rh3t_ctx* ctx, int32_t k, const double* value, double time);
+int rh3t_download_instance(rh3t_ctx* ctx, int32_t k, double* value, double* time);
+/* rh3t_l of instance k */
+int rh3t_l_instance(rh3t_ctx* ctx, int32_t k, double* rhs, double* ghost_values);
+/* calc_global_dt of every instance, dt_cfl[n] */
+int rh3t_calc_global_dt_batch(rh3t_ctx* ctx, double* dt_cfl);
+/* per-instance time, dt of the last step and steps taken (arrays of n, each may be NULL) */
+int rh3t_instance_times(rh3t_ctx* ctx, double* t, double* dt, int64_t* steps);
+/* per-instance status of the last synchronising call (codes[n]) */
+int rh3t_instance_status(const rh3t_ctx* ctx, int32_t* codes);
+
+/* Work-tile shapes (no reference counterpart). Each instance has three
+ * shapes, given as log2 of the tile's j extent: x-face tiles of
+ * (64 >> lg_fx) x (1 << lg_fx) faces, lg_fx in [2, 4]; y-face tiles of
+ * (64 >> lg_fy) x (1 << lg_fy) faces, lg_fy in [4, 6]; RHS tiles of
+ * (256 >> lg_rhs) x (1 << lg_rhs) cells, lg_rhs in [4, 6]. Shapes change
+ * only the work decomposition: results are bit-identical for every shape.
+ * k = -1 sets every instance. */
+int rh3t_set_tile_shapes(rh3t_ctx* ctx, int32_t k, int32_t lg_fx, int32_t lg_fy, int32_t lg_rhs);
+int rh3t_get_tile_shapes(const rh3t_ctx* ctx, int32_t k, int32_t* lg3);
+
+/* Autotuner: instances are grouped into classes by (nx, ny, diffusion on);
+ * for each class every admissible shape of each of the three tile kinds is
+ * timed on the class's own instances (CUDA events, `reps` launches, the
+ * minimum kept) and the fastest is applied. Results are cached per class in
+ * the process and, when cache_path is not NULL, in that text file (read
+ * first, rewritten after). out (may be NULL) receives up to max_out
+ * entries, one per class. Time it after uploading a state. */
+typedef struct {
+    int32_t nx, ny, diffusion, n_instances;
+    int32_t lg_fx, lg_fy, lg_rhs;
+    int32_t from_cache;
+    double ms_fx[3], ms_fy[3], ms_rhs[3]; /* per admissible shape, ascending lg; 0 if from cache */
+} rh3t_tune_entry;
+int rh3t_autotune(rh3t_ctx* ctx, const char* cache_path, int32_t reps, rh3t_tune_entry* out, int32_t max_out,
+                  int32_t* n_out);
 
 /* Field::value host <-> device (values of non-fluid cells are ignored on
  * upload and returned as 0 on download), plus Field::time. */

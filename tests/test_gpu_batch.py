@@ -1,0 +1,162 @@
+"""Batched solver (rh3t_batch_create): uneven instances advanced together.
+
+  - every instance of a batch equals, bit for bit, the same instance advanced
+    alone by the plain solver (the batch changes the work decomposition, not
+    the arithmetic), with its own dt sequence and time;
+  - seeded half-cylinder instances of uneven size, Mach number and exchange
+    coefficients (cases.batch_specs) match the oracle run instance by
+    instance (rel. L-inf, tests/helpers.py rel_linf: <= 1e-10 for the
+    no-contraction build, within the oracle's own FMA envelope otherwise);
+  - every admissible tile shape, and the autotuner's choice, gives
+    bit-identical results;
+  - a failing instance is reported with its index and leaves the others
+    running.
+"""
+import numpy as np
+import pytest
+
+from helpers import rel_linf
+
+pytestmark = pytest.mark.gpu
+
+
+def _mixed_fields(rh):
+    diff = dict(kappa_e=1e-3, kappa_i=1e-3, kappa_r=1e-3, omega_ei=1.0, omega_er=1.0, periodic_ly=0.03125)
+    return [
+        rh.cases.init_cylinder(h=1.0 / 10.0),
+        rh.cases.init_cylinder(h=1.0 / 20.0, mach=2.5, params=rh.Params(omega_ei=0.5, omega_er=2.0)),
+        rh.cases.planar_shock(nx=256, params=rh.Params(**diff)),
+        rh.cases.init_double_mach(h=1.0 / 40.0),
+        rh.cases.init_cylinder(h=1.0 / 10.0, mach=3.7),
+    ]
+
+
+def _alone(rh, f, g, nsteps, exact=False):
+    s = rh.Solver(f, g, exact=exact)
+    s.advance(nsteps, 0.05)
+    u, t = s.download()
+    dt = s.last_dt()
+    s.close()
+    return u, t, dt
+
+
+@pytest.mark.parametrize("exact", [False, True])
+def test_batch_equals_plain_bitwise(rh, exact):
+    fields = _mixed_fields(rh)
+    grids = [rh.GhostGrid.build(f) for f in fields]
+    b = rh.Batch(fields, grids, exact=exact)
+    b.advance(15, 0.05)
+    res = b.download()
+    t, dt, steps = b.times()
+    assert (steps == 15).all()
+    for k, (f, g) in enumerate(zip(fields, grids)):
+        u, tk, dtk = _alone(rh, f, g, 15, exact)
+        assert np.array_equal(res[k][0], u), f"instance {k}"
+        assert res[k][1] == tk == t[k] and dt[k] == dtk
+    assert len(set(t.tolist())) > 1  # per-instance dt: the times differ
+
+
+def test_batch_l_and_dt_per_instance(rh):
+    fields = _mixed_fields(rh)
+    grids = [rh.GhostGrid.build(f) for f in fields]
+    b = rh.Batch(fields, grids)
+    b.advance(5, 0.05)
+    dts = b.calc_global_dt()
+    for k, (f, g) in enumerate(zip(fields, grids)):
+        s = rh.Solver(f, g)
+        s.advance(5, 0.05)
+        assert s.calc_global_dt() == dts[k]
+        r1, g1 = s.l(with_ghosts=True)
+        r2, g2 = b.l(k, with_ghosts=True)
+        assert np.array_equal(r1, r2) and np.array_equal(g1, g2)
+        s.close()
+
+
+@pytest.mark.parametrize("exact", [True, False])
+def test_seeded_batch_matches_oracle(rh, O, exact):
+    """With the exchange source on, these half-cylinders are ill-conditioned:
+    the oracle compiled with FMA contraction differs from itself without by
+    up to ~1e-5 after 20 steps (sign flips of the transverse characteristic
+    speeds on the y = +-6 FarField sides, bc1.rs:829-924, amplified by the
+    stiff exchange terms). The no-contraction build must match the oracle to
+    1e-10; the FMA build must stay within that envelope."""
+    specs = rh.cases.batch_specs(n=4, sizes=(31, 61, 91))
+    fields = [rh.cases.batch_field(sp) for sp in specs]
+    grids = [rh.GhostGrid.build(f) for f in fields]
+    b = rh.Batch(fields, grids, exact=exact)
+    b.advance(20, 0.05)
+    res = b.download()
+    OF = None if exact else O.fma_variant()
+    for k, sp in enumerate(specs):
+        kw = dict(h=sp["h"], mach=sp["mach"], omega_ei=sp["omega_ei"], omega_er=sp["omega_er"])
+        ref = O.Case.cylinder(**kw)
+        assert np.array_equal(fields[k].value, ref.state())
+        ref.run(20, 0.05)
+        err = rel_linf(res[k][0], ref.state(), fields[k].fluid)
+        tol = 1e-10
+        if not exact:
+            ref_fma = OF.Case.cylinder(**kw)
+            ref_fma.run(20, 0.05)
+            tol = max(tol, 2.0 * rel_linf(ref_fma.state(), ref.state(), fields[k].fluid).max())
+        print(f"instance {k} nx={sp['nx']} M={sp['mach']:.3f} exact={exact}: max {err.max():.3e} (tol {tol:.2e})")
+        assert err.max() <= tol
+        assert abs(res[k][1] - ref.time) <= 1e-9 * ref.time
+
+
+def test_tile_shapes_bit_identical(rh):
+    fields = _mixed_fields(rh)[:3]
+    grids = [rh.GhostGrid.build(f) for f in fields]
+    base = rh.Batch(fields, grids)
+    base.advance(6, 0.05)
+    ref, _ = base.download_values()
+    shapes = [(2, 4, 4), (4, 5, 6), (3, 6, 5), (4, 4, 4), (2, 6, 6)]
+    for sh in shapes:
+        b = rh.Batch(fields, grids)
+        b.set_tile_shapes(*sh)
+        assert b.tile_shapes(0) == sh
+        b.advance(6, 0.05)
+        v, _ = b.download_values()
+        assert np.array_equal(v, ref), sh
+    # one instance on its own shape, the others on the default: one launch mixes shapes
+    b = rh.Batch(fields, grids)
+    b.set_tile_shapes(4, 4, 6, k=1)
+    b.advance(6, 0.05)
+    assert np.array_equal(b.download_values()[0], ref)
+
+
+def test_autotune_applies_and_caches(rh, tmp_path):
+    fields = _mixed_fields(rh)
+    grids = [rh.GhostGrid.build(f) for f in fields]
+    b = rh.Batch(fields, grids)
+    cache = str(tmp_path / "tiles.txt")
+    res = b.autotune(cache_path=cache, reps=3)
+    assert len(res) == 4  # two instances share (31, 121, no diffusion)
+    for e in res:
+        assert 2 <= e["shape"][0] <= 4 and 4 <= e["shape"][1] <= 6 and 4 <= e["shape"][2] <= 6
+        assert not e["from_cache"] and min(e["ms_fx"]) > 0
+    b.advance(6, 0.05)
+    v, _ = b.download_values()
+    ref = rh.Batch(fields, grids)
+    ref.advance(6, 0.05)
+    assert np.array_equal(v, ref.download_values()[0])
+    again = rh.Batch(fields, grids).autotune(cache_path=cache)
+    assert all(e["from_cache"] for e in again)
+    assert [e["shape"] for e in again] == [e["shape"] for e in res]
+
+
+def test_failing_instance_isolated(rh):
+    fields = _mixed_fields(rh)[:3]
+    grids = [rh.GhostGrid.build(f) for f in fields]
+    bad = fields[1]
+    k = np.flatnonzero(bad.fluid)[200]
+    bad.value[k, 0] = -1.0  # negative density in one cell of instance 1, injected on the host
+    b = rh.Batch(fields, grids)
+    with pytest.raises(rh.RH3TError) as ei:
+        b.advance(4, 0.05)
+    assert ei.value.instance == 1
+    st = b.status()
+    assert st[1] != 0 and st[0] == 0 and st[2] == 0
+    res = b.download()
+    for q in (0, 2):
+        u, t, _ = _alone(rh, fields[q], grids[q], 4)
+        assert np.array_equal(res[q][0], u) and res[q][1] == t
