@@ -23,7 +23,7 @@ EXPORTS = (
     "rh3t_destroy", "rh3t_batch_create", "rh3t_instance_count", "rh3t_upload_batch", "rh3t_download_batch",
     "rh3t_upload_instance", "rh3t_download_instance", "rh3t_l_instance", "rh3t_calc_global_dt_batch",
     "rh3t_instance_times", "rh3t_instance_status", "rh3t_set_tile_shapes", "rh3t_get_tile_shapes",
-    "rh3t_autotune",
+    "rh3t_autotune", "rh3t_l_vjp", "rh3t_adjoint_forward", "rh3t_adjoint_backward",
 )
 
 
@@ -133,6 +133,9 @@ def load(exact=False):
         "rh3t_set_tile_shapes": (I, [V, C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
         "rh3t_get_tile_shapes": (I, [V, C.c_int32, V]),
         "rh3t_autotune": (I, [V, C.c_char_p, C.c_int32, V, C.c_int32, P(C.c_int32)]),
+        "rh3t_l_vjp": (I, [V, C.c_int32, V, V, V]),
+        "rh3t_adjoint_forward": (I, [V, C.c_int32, D, C.c_int32]),
+        "rh3t_adjoint_backward": (I, [V, V, V, V]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

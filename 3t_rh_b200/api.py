@@ -578,6 +578,32 @@ class Batch:
         self._check(self.L.rh3t_profile_steps(self.h, int(nsteps), float(cfl_factor), ms.ctypes.data, cnt.ctypes.data))
         return dict(zip(("ghosts", "flux", "rhs_stage", "dt"), zip(ms.tolist(), cnt.tolist())))
 
+    # ---- adjoint (no reference counterpart)
+    def l_vjp(self, k, rbar):
+        """Cotangent of instance k's resident state for a cotangent rbar of
+        its l() (nx*ny x 6); returns (ubar, pbar) with pbar = (FarField state
+        (6), omega_ei, omega_er)."""
+        rb = _arr(rbar, np.float64)
+        ub = np.zeros((int(self.cells[k]), 6))
+        pb = np.zeros(8)
+        self._check(self.L.rh3t_l_vjp(self.h, int(k), rb.ctypes.data, ub.ctypes.data, pb.ctypes.data))
+        return ub, pb
+
+    def adjoint_forward(self, nsteps, cfl_factor=0.05, ckpt_every=20):
+        """nsteps steps of every instance with checkpoints every ckpt_every."""
+        self._check(self.L.rh3t_adjoint_forward(self.h, int(nsteps), float(cfl_factor), int(ckpt_every)))
+
+    def adjoint_backward(self, dJ_du):
+        """dJ_du: per-instance list of (nx*ny x 6) arrays or their
+        concatenation. Returns ([dJ/du0 per instance], dJ/dparams (n x 8))."""
+        if isinstance(dJ_du, (list, tuple)):
+            dJ_du = np.concatenate([_arr(x, np.float64).reshape(-1, 6) for x in dJ_du])
+        lam = _arr(dJ_du, np.float64)
+        g0 = np.zeros((int(self.offsets[-1]), 6))
+        gp = np.zeros((self.n, 8))
+        self._check(self.L.rh3t_adjoint_backward(self.h, lam.ctypes.data, g0.ctypes.data, gp.ctypes.data))
+        return [g0[self.offsets[k]:self.offsets[k + 1]] for k in range(self.n)], gp
+
     def synchronize(self):
         self._check(self.L.rh3t_synchronize(self.h))
 

@@ -9,6 +9,8 @@ keeps in init.rs, restated for inputs of the solver).
   batch_specs       seeded half-cylinder instances of uneven size and
                     parameters for the batched solver (the LCG of the
                     reference's parity tests, main.rs:493-498)
+  SurfacePressure   the adjoint's objective: pressure integrated over the
+                    cylinder arc (no reference counterpart)
 """
 import math
 
@@ -195,3 +197,54 @@ def batch_field(spec):
     """The half-cylinder Field of one batch_specs entry."""
     return init_cylinder(h=spec["h"], mach=spec["mach"],
                          params=Params(omega_ei=spec["omega_ei"], omega_er=spec["omega_er"]))
+
+
+# ------------------------------------------------------------------ adjoint objective
+class SurfacePressure:
+    """J(u) = h * sum over the ghosts of the arc sides of p(u[n_g]), n_g the
+    fluid node nearest to the ghost's boundary foot P0 (among the 3 x 3 nodes
+    around its rounded grid index), p = p_e + p_i + p_r (state.rs:245-276) and
+    h = sqrt(dx dy): the surface pressure integral on the cylinder, each
+    ghost standing for one arc element of length h."""
+
+    def __init__(self, field, ghosts, arc=0):
+        g = field.grid
+        a = field.outer_arcs[arc]
+        sel = (ghosts.boundary == 0) & (ghosts.side >= a.side_start) & (ghosts.side <= a.side_end)
+        nodes = []
+        for p0x, p0y in ghosts.proj[sel, :2]:
+            ic, jc = _round((p0x - g.x0) / g.dx), _round((p0y - g.y0) / g.dy)
+            best, bn = math.inf, None
+            for di in (0, -1, 1):
+                for dj in (0, -1, 1):
+                    i, j = int(ic) + di, int(jc) + dj
+                    if 0 <= i < g.nx and 0 <= j < g.ny and field.fluid[i * g.ny + j]:
+                        d2 = (g.x0 + i * g.dx - p0x) ** 2 + (g.y0 + j * g.dy - p0y) ** 2
+                        if d2 < best:
+                            best, bn = d2, i * g.ny + j
+            if bn is None:
+                raise ValueError("arc ghost without a fluid node near its foot")
+            nodes.append(bn)
+        self.nodes = np.array(nodes, np.int64)
+        self.h = math.sqrt(g.dx * g.dy)
+        P = field.params
+        self.g3 = np.array([P.gamma_e - 1.0, P.gamma_i - 1.0, P.gamma_r - 1.0])
+
+    def value(self, u):
+        s = np.asarray(u)[self.nodes]
+        rw2 = (s[:, 1] ** 2 + s[:, 2] ** 2) / s[:, 0]
+        p = (self.g3[None, :] * (s[:, 3:6] - rw2[:, None] / 6.0)).sum(1)
+        return self.h * p.sum()
+
+    def grad(self, u):
+        u = np.asarray(u)
+        s = u[self.nodes]
+        G = self.g3.sum()
+        gp = np.zeros_like(s)
+        gp[:, 0] = G * (s[:, 1] ** 2 + s[:, 2] ** 2) / (6.0 * s[:, 0] ** 2)
+        gp[:, 1] = -G * s[:, 1] / (3.0 * s[:, 0])
+        gp[:, 2] = -G * s[:, 2] / (3.0 * s[:, 0])
+        gp[:, 3:6] = self.g3[None, :]
+        out = np.zeros_like(u)
+        np.add.at(out, self.nodes, self.h * gp)
+        return out

@@ -296,6 +296,7 @@ int build_instance(const rh3t_instance& d, int inst, HostInst& H, Inst& I, Built
         R.ny = gt->proj[5 * g + 3]; R.dist = gt->proj[5 * g + 4];
         R.heavy = -1;
         const int kind = R.kind;
+        if (kind == BC_WALL || kind == BC_OUTFLOW) H.adj_unsupported = true;
         if (kind == BC_WALL || kind == BC_OUTFLOW || kind == BC_FAR_FIELD) {
             int k = gt->pre[g];
             if (k < 0 || k >= nh) {
@@ -572,6 +573,9 @@ extern "C" int rh3t_batch_create(int32_t n, const rh3t_instance* desc, int32_t d
         off_bcs[k] = n_bcs; n_bcs += B[k].bcs.size();
         H.cell_off = c->total_cells;
         I.cell_off = H.cell_off;
+        I.aoff = c->total_planes;
+        c->total_planes += 6 * H.plane;
+        c->max_faces = std::max(c->max_faces, std::max((long long)(H.nx + 1) * H.ny, (long long)H.nx * (H.ny + 1)));
         c->total_cells += H.nx * H.ny;
         c->max_cells = std::max(c->max_cells, (long long)H.nx * H.ny);
         H.ghost_off = ghost_base;
@@ -697,6 +701,7 @@ extern "C" void rh3t_destroy(rh3t_ctx* c) {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    adj_free(c);
     if (c->graph) cudaGraphExecDestroy(c->graph);
     dfree(c->d_state); dfree(c->d_mask); dfree(c->d_faces); dfree(c->d_bcs); dfree(c->d_sc); dfree(c->d_err);
     dfree(c->d_times); dfree(c->d_inst); dfree(c->d_ghosts); dfree(c->d_gpart); dfree(c->d_hrec);

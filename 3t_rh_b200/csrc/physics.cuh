@@ -9,7 +9,7 @@
 
 namespace rh3t {
 
-__device__ __forceinline__ double sqd(double x) { return x * x; }
+template <class T> __device__ __forceinline__ T sqd(T x) { return x * x; }
 __device__ __forceinline__ double pow4d(double x) { return (x * x) * (x * x); }
 
 // ---- correctly rounded powers for the two pow() calls of the reference
@@ -118,9 +118,10 @@ __device__ __forceinline__ void phys_flux(const double s[6], const Prim& d, doub
 
 // Roe (sqrt(rho)-weighted) averages shared by weno.rs:28-78 build_l_plain and
 // weno.rs:484-516 build_r_plain (state1 = points[3], state2 = points[2]).
-struct Roe {
-    double u, v, w2, ee, ei, er, cs2, cs, he, hi, hr, b, den;
+template <class T> struct RoeT {
+    T u, v, w2, ee, ei, er, cs2, cs, he, hi, hr, b, den;
 };
+using Roe = RoeT<double>;
 
 __device__ __forceinline__ Roe roe_average(double rho_s1, const Prim& d3, double rho_s2, const Prim& d2,
                                            const DevParams& P) {
@@ -148,12 +149,13 @@ __device__ __forceinline__ Roe roe_average(double rho_s1, const Prim& d3, double
 
 // Row `row` of the left eigenvector matrix (weno.rs:79-458). DIR 0: rows
 // [u-c, e, i, r, transverse, u+c]; DIR 1: [v-c, transverse, e, i, r, v+c].
-template <int DIR>
-__device__ __forceinline__ void l_row(int row, const Roe& q, const DevParams& P, double L[6]) {
+// Written over the scalar type T (double; a dual-number type in the adjoint).
+template <int DIR, class T>
+__device__ __forceinline__ void l_row(int row, const RoeT<T>& q, const DevParams& P, T L[6]) {
     const double GE = P.gamma_e, GI = P.gamma_i, GR = P.gamma_r;
     const double gi = GI - 1.0, ge = GE - 1.0, gr = GR - 1.0;
     const double gt = gi + ge + gr;
-    const double u = q.u, v = q.v, w2 = q.w2, cs = q.cs, cs2 = q.cs2, b = q.b, den = q.den;
+    const T u = q.u, v = q.v, w2 = q.w2, cs = q.cs, cs2 = q.cs2, b = q.b, den = q.den;
     // map to a mode: 0 acoustic-, 1 transverse, 2 electron, 3 ion, 4 radiation, 5 acoustic+
     int mode;
     if (DIR == 0) {
@@ -179,11 +181,11 @@ __device__ __forceinline__ void l_row(int row, const Roe& q, const DevParams& P,
         L[4] = 6.0 * gi / den;
         L[5] = 6.0 * gr / den;
     } else if (mode == 1) {
-        if (DIR == 0) { L[0] = -v; L[1] = 0.0; L[2] = 1.0; }
-        else { L[0] = -u; L[1] = 1.0; L[2] = 0.0; }
-        L[3] = 0.0; L[4] = 0.0; L[5] = 0.0;
+        if (DIR == 0) { L[0] = -v; L[1] = T(0.0); L[2] = T(1.0); }
+        else { L[0] = -u; L[1] = T(1.0); L[2] = T(0.0); }
+        L[3] = T(0.0); L[4] = T(0.0); L[5] = T(0.0);
     } else if (mode == 2) {
-        const double he = q.he;
+        const T he = q.he;
         L[0] = ge / gt - ge * w2 / (6.0 * cs2) - ge * gt * w2 / b * (he - cs2 * w2);
         L[1] = ge * u / (3.0 * cs2) + 2.0 * ge * gt * u / b * (he - cs2 * w2);
         L[2] = ge * v / (3.0 * cs2) + 2.0 * ge * gt * v / b * (he - cs2 * w2);
@@ -191,7 +193,7 @@ __device__ __forceinline__ void l_row(int row, const Roe& q, const DevParams& P,
         L[4] = -ge * gi / (gt * cs2) - 6.0 * ge * gi / b * (he - 6.0 * gr * cs2);
         L[5] = -ge * gr / (gt * cs2) - 6.0 * ge * gr / b * (he + 6.0 * gi * cs2);
     } else if (mode == 3) {
-        const double hi = q.hi;
+        const T hi = q.hi;
         L[0] = gi / gt - gi * w2 / (6.0 * cs2) - gi * gt * w2 / b * (hi - cs2 * w2);
         L[1] = gi * u / (3.0 * cs2) + 2.0 * gi * gt * u / b * (hi - cs2 * w2);
         L[2] = gi * v / (3.0 * cs2) + 2.0 * gi * gt * v / b * (hi - cs2 * w2);
@@ -199,7 +201,7 @@ __device__ __forceinline__ void l_row(int row, const Roe& q, const DevParams& P,
         L[4] = -sqd(gi) / (gt * cs2) - 6.0 * gi / b * (gi * hi - gt * cs2 * w2);
         L[5] = -gi * gr / (gt * cs2) - 6.0 * gi * gr / b * (hi - 6.0 * ge * cs2);
     } else {
-        const double hr = q.hr;
+        const T hr = q.hr;
         L[0] = gr / gt - gr * w2 / (6.0 * cs2) - gr * gt * w2 / b * (hr - cs2 * w2);
         L[1] = gr * u / (3.0 * cs2) + 2.0 * gr * gt * u / b * (hr - cs2 * w2);
         L[2] = gr * v / (3.0 * cs2) + 2.0 * gr * gt * v / b * (hr - cs2 * w2);
@@ -210,12 +212,12 @@ __device__ __forceinline__ void l_row(int row, const Roe& q, const DevParams& P,
 }
 
 // Column `col` of the right eigenvector matrix and eigenvalue (weno.rs:518-545).
-template <int DIR>
-__device__ __forceinline__ void r_col(int col, const Roe& q, const DevParams& P, double R[6], double& lam) {
+template <int DIR, class T>
+__device__ __forceinline__ void r_col(int col, const RoeT<T>& q, const DevParams& P, T R[6], T& lam) {
     const double GE = P.gamma_e, GI = P.gamma_i, GR = P.gamma_r;
     const double gi = GI - 1.0, ge = GE - 1.0, gr = GR - 1.0;
     const double gt = gi + ge + gr;
-    const double u = q.u, v = q.v, w2 = q.w2, cs = q.cs;
+    const T u = q.u, v = q.v, w2 = q.w2, cs = q.cs;
     if (DIR == 0) {
         switch (col) {
         case 0:
@@ -487,28 +489,34 @@ __device__ __forceinline__ void noncon9(const double pe[9], const double pi[9], 
     out[2] = v / 3.0 * der_er + (coef_left * jm_er + coef_right * jp_er) / ds;
 }
 
-// dt.rs:5-34 get_local_dt (same association order; CVE^3 = CVE*(CVE*CVE))
-__device__ __forceinline__ double local_dt(const double s[6], double dx, double dy, const DevParams& P) {
-    double u = s[1] / s[0], v = s[2] / s[0];
-    double ee = s[3] / s[0] - (sqd(u) + sqd(v)) / 6.0;
-    double ei = s[4] / s[0] - (sqd(u) + sqd(v)) / 6.0;
-    double er = s[5] / s[0] - (sqd(u) + sqd(v)) / 6.0;
+// dt.rs:5-34 get_local_dt (same association order; CVE^3 = CVE*(CVE*CVE)),
+// over the scalar type T with the exchange coefficients as arguments (the
+// adjoint differentiates it in the state and in them)
+template <class T>
+__device__ __forceinline__ T local_dt_t(const T s[6], double dx, double dy, const DevParams& P, T OEI, T OER) {
+    T u = s[1] / s[0], v = s[2] / s[0];
+    T ee = s[3] / s[0] - (sqd(u) + sqd(v)) / 6.0;
+    T ei = s[4] / s[0] - (sqd(u) + sqd(v)) / 6.0;
+    T er = s[5] / s[0] - (sqd(u) + sqd(v)) / 6.0;
     const double GE = P.gamma_e, GI = P.gamma_i, GR = P.gamma_r, A = P.a_rad, CVE = P.cve, CVI = P.cvi;
-    const double OEI = P.omega_ei, OER = P.omega_er;
     const double gi = GI - 1.0, ge = GE - 1.0, gr = GR - 1.0;
-    double cs = sqrt(GE * ge * ee + GI * gi * ei + GR * gr * er);
+    T cs = sqrt(GE * ge * ee + GI * gi * ei + GR * gr * er);
     const double c4 = (CVE * CVE) * (CVE * CVE), c3 = CVE * (CVE * CVE);
-    double ee3 = ee * (ee * ee);
-    double t1 = A * OEI * c4 + A * OEI * c3 * CVI + 4.0 * A * OER * CVI * ee3 + OER * c4 * CVI * s[0];
-    double s1 = sqrt(sqd(t1) - 4.0 * A * OEI * OER * c4 * CVI * (4.0 * A * ee3 + c4 * s[0] + c3 * CVI * s[0]));
-    double s2 = -(A * OEI * c4 + A * OEI * c3 * CVI + 4.0 * A * OER * CVI * ee3 + OER * c4 * CVI * s[0]);
-    double sden = 2.0 * A * c4 * CVI * s[0];
-    double alpha1 = fabs((-s1 + s2) / sden);
-    double alpha2 = fabs((s1 + s2) / sden);
-    double sj = fmax(alpha1, alpha2);
-    double dj = fmax(fmax(P.kappa_e / (CVE * s[0]), P.kappa_i / (CVI * s[0])), P.kappa_r / A);
-    double vj = (fabs(u) + cs) / dx + 2.0 * dj / (sqd(dx) + sqd(dy)) + sj + (fabs(v) + cs) / dy;
+    T ee3 = ee * (ee * ee);
+    T t1 = A * OEI * c4 + A * OEI * c3 * CVI + 4.0 * A * OER * CVI * ee3 + OER * c4 * CVI * s[0];
+    T s1 = sqrt(sqd(t1) - 4.0 * A * OEI * OER * c4 * CVI * (4.0 * A * ee3 + c4 * s[0] + c3 * CVI * s[0]));
+    T s2 = -(A * OEI * c4 + A * OEI * c3 * CVI + 4.0 * A * OER * CVI * ee3 + OER * c4 * CVI * s[0]);
+    T sden = 2.0 * A * c4 * CVI * s[0];
+    T alpha1 = fabs((-s1 + s2) / sden);
+    T alpha2 = fabs((s1 + s2) / sden);
+    T sj = fmax(alpha1, alpha2);
+    T dj = fmax(fmax(P.kappa_e / (CVE * s[0]), P.kappa_i / (CVI * s[0])), T(P.kappa_r / A));
+    T vj = (fabs(u) + cs) / dx + 2.0 * dj / (sqd(dx) + sqd(dy)) + sj + (fabs(v) + cs) / dy;
     return P.lambda / vj;
+}
+
+__device__ __forceinline__ double local_dt(const double s[6], double dx, double dy, const DevParams& P) {
+    return local_dt_t<double>(s, dx, dy, P, P.omega_ei, P.omega_er);
 }
 
 namespace fastm {

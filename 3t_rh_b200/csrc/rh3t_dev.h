@@ -86,6 +86,7 @@ struct Inst {
     int32_t nx, ny, nyp, n_tiles_dt;
     long long plane;                // (nx + 2*PAD) * nyp
     long long cell_off;             // sum of nx*ny over the instances before this one
+    long long aoff;                 // sum of 6*plane before this one: offset in batch-wide plane sets
     double dx, dy;
     DevParams P;
     int32_t diffusion, source;

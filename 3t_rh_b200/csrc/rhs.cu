@@ -10,7 +10,9 @@
 // evaluate them once per use, 17 times per node.
 //
 // mode 0 writes the rhs (6 planes of nx*ny, i*ny+j, instance k at
-// rhs_out + 6*cell_off) for l(); mode 1 applies the stage update of `stage`.
+// rhs_out + 6*cell_off) for l(); mode 1 applies the stage update of `stage`;
+// mode 2 does both, the rhs into padded planes at rhs_out + aoff (the
+// adjoint's record of the forward stages).
 #include "common.cuh"
 #include "kernels.cuh"
 #include "physics.cuh"
@@ -107,6 +109,11 @@ __global__ void __launch_bounds__(RHS_THREADS) k_rhs_stage(const Inst* __restric
 #pragma unroll
         for (int c = 0; c < 6; ++c) ro[c * lp + ln] = rhs[c];
         return;
+    }
+    if (mode == 2) {
+        double* __restrict__ ro = rhs_out + I.aoff;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) ro[c * plane + n] = rhs[c];
     }
     const DevScalars& sc = *I.sc;
     double v[6];

@@ -236,6 +236,29 @@ typedef struct {
 int rh3t_autotune(rh3t_ctx* ctx, const char* cache_path, int32_t reps, rh3t_tune_entry* out, int32_t max_out,
                   int32_t* n_out);
 
+/* Adjoint (no reference counterpart: the reference has no derivative
+ * code). Hand-written vector-Jacobian products of l() and of the SSP-RK3
+ * step, for instances whose ghosts are FarField, ReflectiveWall, ZerothOrder,
+ * Periodic, Constant or TimeDependent (Wall and Outflow are rejected with
+ * RH3T_ERR_INVALID_ARGUMENT). Kinks follow the values: d|x|/dx = +1 at 0,
+ * max/min pass the derivative to the first argument on ties, FarField rows
+ * switch on lambda < 0, dt's derivative goes to the first minimising cell.
+ * Parameter cotangents per instance (8 doubles): the FarField state (6, one
+ * for all FarField sides), omega_ei, omega_er. */
+/* rbar: nx*ny*6 cotangent of l()'s result for instance k; ubar (out): the
+ * cotangent of the resident state, pbar8 (out, may be NULL). */
+int rh3t_l_vjp(rh3t_ctx* ctx, int32_t k, const double* rbar, double* ubar, double* pbar8);
+/* Runs nsteps steps of every instance (dt = cfl_factor * dt_cfl, no
+ * clipping) from the resident states, saving the states every ckpt_every
+ * steps for rh3t_adjoint_backward. */
+int rh3t_adjoint_forward(rh3t_ctx* ctx, int32_t nsteps, double cfl_factor, int32_t ckpt_every);
+/* dJ_du: cotangent of the final states (all instances' value arrays
+ * concatenated); dJ_du0 (out, same layout): gradient with respect to the
+ * initial states; dJ_dparams (out, n x 8, may be NULL). Recomputes each
+ * segment from its checkpoint; the resident states are those at the end of
+ * the forward run afterwards. */
+int rh3t_adjoint_backward(rh3t_ctx* ctx, const double* dJ_du, double* dJ_du0, double* dJ_dparams);
+
 /* Field::value host <-> device (values of non-fluid cells are ignored on
  * upload and returned as 0 on download), plus Field::time. */
 int rh3t_upload_state(rh3t_ctx* ctx, const double* value, double time);

@@ -71,6 +71,8 @@ def lib():
             ("oracle_access", None, [P, C.c_void_p]),
             ("oracle_last_error", I, [P, C.c_void_p, C.c_char_p, I]),
             ("oracle_l", I, [P, C.c_void_p, C.c_void_p]),
+            ("oracle_l_jvp", I, [P] + [C.c_void_p] * 7),
+            ("oracle_l_t", I, [P, C.c_void_p, C.c_void_p]),
             ("oracle_rk3", I, [P, D]),
             ("oracle_global_dt", D, [P]),
             ("oracle_run", I, [P, LG, D, C.c_void_p]),
@@ -105,6 +107,10 @@ def lib():
             f.argtypes = args
         _lib = L
     return _lib
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data
 
 
 def _dp(a):
@@ -258,6 +264,27 @@ class Case:
         rhs = np.zeros((self.n, 6))
         gv = np.zeros((self.n_ghosts(), 6))
         self._check(lib().oracle_l(self.h, rhs.ctypes.data, gv.ctypes.data))
+        return rhs, gv
+
+    def l_jvp(self, du=None, duinf=None, domega=None):
+        """Forward-mode directional derivative of l() (dual numbers): returns
+        (rhs, d rhs, ghost values, d ghost values) for a state direction du
+        (nx*ny x 6), a direction of every FarField state (6) and of
+        (omega_ei, omega_er)."""
+        rhs, drhs = np.zeros((self.n, 6)), np.zeros((self.n, 6))
+        gv, dgv = np.zeros((self.n_ghosts(), 6)), np.zeros((self.n_ghosts(), 6))
+        du = None if du is None else np.ascontiguousarray(du, np.float64)
+        du6 = None if duinf is None else np.ascontiguousarray(duinf, np.float64)
+        dom = None if domega is None else np.ascontiguousarray(domega, np.float64)
+        self._check(lib().oracle_l_jvp(self.h, _ptr(du), _ptr(du6), _ptr(dom), rhs.ctypes.data, drhs.ctypes.data,
+                                       gv.ctypes.data, dgv.ctypes.data))
+        return rhs, drhs, gv, dgv
+
+    def l_t(self):
+        """l() through the scalar-type templates at T = double"""
+        rhs = np.zeros((self.n, 6))
+        gv = np.zeros((self.n_ghosts(), 6))
+        self._check(lib().oracle_l_t(self.h, rhs.ctypes.data, gv.ctypes.data))
         return rhs, gv
 
     def rk3_ssp(self, dt):

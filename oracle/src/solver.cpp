@@ -5,6 +5,7 @@
 // conditions of init.rs, and a C API used by the Python tests and bench.
 // OpenMP loops stand where the reference has Rayon par_iter loops.
 #include "model.hpp"
+#include "jvp.hpp"
 #include <algorithm>
 #include <atomic>
 #include <cmath>
@@ -653,6 +654,323 @@ static void init_rect(Field& u, long nx, long ny, double lx, double ly, const St
     u.value.assign(u.grid.len(), value);
 }
 
+
+// ---------------------------------------------------------------- l() over a scalar type
+// The functions above written over T (jvp.hpp): same operations, same order.
+template <class T> static bool solve6_t(T A[6][6], T b[6]) {
+    int piv[6];
+    for (int j = 0; j < 6; ++j) {
+        int p = j;
+        double mx = std::fabs(val(A[j][j]));
+        for (int i = j + 1; i < 6; ++i)
+            if (std::fabs(val(A[i][j])) > mx) { mx = std::fabs(val(A[i][j])); p = i; }
+        piv[j] = p;
+        if (val(A[p][j]) == 0.0) return false;
+        if (p != j) for (int k = 0; k < 6; ++k) std::swap(A[j][k], A[p][k]);
+        T rcp = T(1.0) / A[j][j];
+        for (int i = j + 1; i < 6; ++i) A[i][j] *= rcp;
+        for (int k = j + 1; k < 6; ++k)
+            for (int i = j + 1; i < 6; ++i) A[i][k] -= A[i][j] * A[j][k];
+    }
+    for (int j = 0; j < 6; ++j) if (piv[j] != j) std::swap(b[j], b[piv[j]]);
+    for (int k = 0; k < 6; ++k)
+        for (int i = k + 1; i < 6; ++i) b[i] -= b[k] * A[i][k];
+    for (int k = 5; k >= 0; --k) {
+        b[k] /= A[k][k];
+        for (int i = 0; i < k; ++i) b[i] -= b[k] * A[i][k];
+    }
+    return true;
+}
+
+template <class T> static void mat_vec_t(const T M[6][6], const T x[6], T out[6]) {
+    for (int i = 0; i < 6; ++i) {
+        T acc = T(0.0);
+        for (int j = 0; j < 6; ++j) acc += M[i][j] * x[j];
+        out[i] = acc;
+    }
+}
+
+template <class T>
+static void build_local_plain_t(Vec2 n, const StateT<T>& val_, const Params& P, T L[6][6], T R[6][6], T lam[6]) {
+    T mom_n = val_.mx * n.x + val_.my * n.y;
+    T mom_t = -val_.mx * n.y + val_.my * n.x;
+    StateT<T> s1{val_.rho, mom_n, mom_t, val_.ee, val_.ei, val_.er};
+    DerivedT<T> d1 = derived_from_state(s1, P);
+    build_l_plain(s1, s1, d1, d1, DIR_X, P, L);
+    build_r_plain(s1, s1, d1, d1, DIR_X, P, lam, R);
+}
+
+template <class T>
+static void weno_extrapolation_all_t(const T L[6][6], const GhostBC& bc, const StateT<T>* v_, const Params& P,
+                                     T v[5][6]) {
+    using std::pow;
+    Vec2 n = bc.normal;
+    T alpha[6][5], vks[5][6][5], asum[6];
+    for (int c = 0; c < 6; ++c) asum[c] = T(0.0);
+    for (int r = 0; r <= 4; ++r) {
+        int m = (r + 1) * (r + 1);
+        T data[6][25];
+        for (int a = 0; a < m; ++a) {
+            const StateT<T>& s = v_[bc.stencil[BC_STENCIL_OFF[r] + a]];
+            T mn = s.mx * n.x + s.my * n.y;
+            T mt = -s.mx * n.y + s.my * n.x;
+            T u6[6] = {s.rho, mn, mt, s.ee, s.ei, s.er};
+            for (int c = 0; c < 6; ++c) {
+                const T* row = L[c];
+                data[c][a] = row[0] * u6[0] + row[1] * u6[1] + row[2] * u6[2] + row[3] * u6[3] + row[4] * u6[4] +
+                             row[5] * u6[5];
+            }
+        }
+        for (int c = 0; c < 6; ++c) {
+            int soff = BC_S_OFF[r];
+            T beta = T(0.0);
+            for (int a = 0; a < m; ++a) {
+                int base = soff + a * m;
+                T acc = T(0.0);
+                for (int b = 0; b < m; ++b) acc += bc.s[base + b] * data[c][b];
+                beta += data[c][a] * acc;
+            }
+            for (int k = 0; k < 5; ++k) {
+                T vk = T(0.0);
+                if (k <= r) {
+                    int woff = BC_W_OFF[r] + k * m;
+                    for (int a = 0; a < m; ++a) vk += bc.w[woff + a] * data[c][a];
+                }
+                vks[k][c][r] = vk;
+            }
+            alpha[c][r] = bc.d[r] / pow(P.eps + beta, P.weno_q);
+            asum[c] += alpha[c][r];
+        }
+    }
+    for (int k = 0; k < 5; ++k)
+        for (int c = 0; c < 6; ++c) {
+            T res = T(0.0);
+            for (int r = 0; r <= 4; ++r) res += (alpha[c][r] / asum[c]) * vks[k][c][r];
+            v[k][c] = res;
+        }
+}
+
+template <class T> static StateT<T> taylor_rotate_t(T u[5][6], double d, Vec2 n) {
+    T g[6];
+    for (int c = 0; c < 6; ++c) g[c] = u[0][c];
+    double coef = 1.0;
+    for (int k = 1; k <= 4; ++k) {
+        coef *= d / (double)k;
+        for (int c = 0; c < 6; ++c) g[c] = g[c] + coef * u[k][c];
+    }
+    T mom_n = g[1], mom_t = g[2];
+    return {g[0], mom_n * n.x - mom_t * n.y, mom_n * n.y + mom_t * n.x, g[3], g[4], g[5]};
+}
+
+template <class T>
+static StateT<T> set_ghost_point_value_t(const GhostInfo& g, const Field& f, const StateT<T>* v_, double t,
+                                         const GhostGrid& gg, const Params& P, const Tangent& tg) {
+    using std::sqrt; using std::fabs;
+    const BC& bc = (g.boundary == OUTER ? f.bc_outer : f.bc_inner)[g.side_id];
+    const Projection& pr = g.project;
+    auto cst = [](const State& s) { return StateT<T>{T(s.rho), T(s.mx), T(s.my), T(s.ee), T(s.ei), T(s.er)}; };
+    switch (bc.kind) {
+    case BC_CONSTANT: return cst(bc.state);
+    case BC_TIME_DEPENDENT: {
+        double xs = bc.td_x0 + bc.td_speed * t;
+        return cst(pr.point.x <= xs ? bc.td_left : bc.td_right);
+    }
+    case BC_REFLECTIVE_WALL: {
+        long oi, oj;
+        if (!mirror_source(g.i, g.j, pr, f, oi, oj))
+            throw OracleError(ERR_GEOMETRY, "cannot find reflected interior point for ghost", g.i, g.j);
+        const StateT<T>& s = v_[f.linear_index(oi, oj)];
+        Vec2 n = pr.normal;
+        T mom_n = s.mx * n.x + s.my * n.y;
+        return {s.rho, s.mx - 2.0 * mom_n * n.x, s.my - 2.0 * mom_n * n.y, s.ee, s.ei, s.er};
+    }
+    case BC_ZEROTH_ORDER: {
+        long oi, oj;
+        if (!mirror_source(g.i, g.j, pr, f, oi, oj))
+            throw OracleError(ERR_GEOMETRY, "cannot find interior point for zeroth-order ghost", g.i, g.j);
+        return v_[f.linear_index(oi, oj)];
+    }
+    case BC_PERIODIC: {
+        long np = (long)std::round(P.periodic_ly / f.grid.dy);
+        long jw = ((g.j % np) + np) % np;
+        if (!f.is_in_domain(g.i, jw)) throw OracleError(ERR_PERIODIC, "periodic wrapped point is not fluid", g.i, jw);
+        return v_[f.linear_index(g.i, jw)];
+    }
+    default: break;
+    }
+    const GhostBC& pre = gg.pre[g.pre];
+    T L[6][6], R[6][6], lam[6];
+    build_local_plain_t(pr.normal, v_[f.linear_index(pre.nearest_i, pre.nearest_j)], P, L, R, lam);
+    T v[5][6];
+    weno_extrapolation_all_t(L, pre, v_, P, v);
+    T u[5][6];
+    if (bc.kind == BC_WALL) {
+        T A0[6][6], rhs0[6];
+        for (int i = 0; i < 6; ++i) for (int c = 0; c < 6; ++c) A0[i][c] = L[i][c];
+        for (int c = 0; c < 6; ++c) A0[0][c] = T(c == 1 ? 1.0 : 0.0);
+        for (int c = 0; c < 6; ++c) rhs0[c] = v[0][c];
+        rhs0[0] = T(0.0);
+        if (!solve6_t(A0, rhs0)) throw OracleError(ERR_SINGULAR, "singular ILW/extrapolation system at boundary", g.i, g.j);
+        for (int c = 0; c < 6; ++c) u[0][c] = rhs0[c];
+        T A1[6][6], rhs1[6], row1[6];
+        for (int i = 0; i < 6; ++i) for (int c = 0; c < 6; ++c) A1[i][c] = L[i][c];
+        double gi = P.gamma_i - 1.0, ge = P.gamma_e - 1.0, gr = P.gamma_r - 1.0;
+        double gt = gi + ge + gr;
+        T u1 = u[0][0], u3 = u[0][2];
+        row1[0] = -gt * sq(u3) / (6.0 * sq(u1));
+        row1[1] = T(0.0);
+        row1[2] = gt * u3 / (6.0 * u1);
+        row1[3] = T(-ge); row1[4] = T(-gi); row1[5] = T(-gr);
+        for (int c = 0; c < 6; ++c) A1[0][c] = row1[c];
+        for (int c = 0; c < 6; ++c) rhs1[c] = v[1][c];
+        rhs1[0] = T(0.0);
+        if (!solve6_t(A1, rhs1)) throw OracleError(ERR_SINGULAR, "singular ILW/extrapolation system at boundary", g.i, g.j);
+        for (int c = 0; c < 6; ++c) u[1][c] = rhs1[c];
+        for (int k = 2; k <= 4; ++k) mat_vec_t(R, v[k], u[k]);
+    } else if (bc.kind == BC_OUTFLOW) {
+        mat_vec_t(R, v[0], u[0]);
+        T rho0 = u[0][0];
+        T un0 = u[0][1] / rho0, ut0 = u[0][2] / rho0;
+        T w2 = un0 * un0 + ut0 * ut0;
+        T ee1 = u[0][3] / rho0 - w2 / 6.0, ei1 = u[0][4] / rho0 - w2 / 6.0, er1 = u[0][5] / rho0 - w2 / 6.0;
+        double ge = P.gamma_e - 1.0, gi = P.gamma_i - 1.0, gr = P.gamma_r - 1.0;
+        T p0 = rho0 * (ge * ee1 + gi * ei1 + gr * er1);
+        T a2 = P.gamma_e * ge * ee1 + P.gamma_i * gi * ei1 + P.gamma_r * gr * er1;
+        T a = sqrt(a2);
+        T lambda1 = un0 - a;
+        T rhs1[6];
+        for (int c = 0; c < 6; ++c) rhs1[c] = v[1][c];
+        if (val(lambda1) < 0.0) {
+            T m_local = fabs(un0 / a);
+            T l1 = bc.sigma * (1.0 - sq(m_local)) * a / bc.l_domain * (p0 - bc.p_inf);
+            rhs1[0] = l1 / lambda1;
+        }
+        mat_vec_t(R, rhs1, u[1]);
+        for (int k = 2; k <= 4; ++k) mat_vec_t(R, v[k], u[k]);
+    } else if (bc.kind == BC_FAR_FIELD) {
+        Vec2 n = pr.normal;
+        StateT<T> ui;
+        for (int c = 0; c < 6; ++c) ui[c] = seed<T>(bc.state[c], tg.duinf[c]);
+        T uinf[6] = {ui.rho, ui.mx * n.x + ui.my * n.y, -ui.mx * n.y + ui.my * n.x, ui.ee, ui.ei, ui.er};
+        T vinf[6];
+        mat_vec_t(L, uinf, vinf);
+        T rhs0[6];
+        for (int c = 0; c < 6; ++c) rhs0[c] = val(lam[c]) < 0.0 ? vinf[c] : v[0][c];
+        mat_vec_t(R, rhs0, u[0]);
+        for (int k = 1; k <= 4; ++k) {
+            T rk[6];
+            for (int c = 0; c < 6; ++c) rk[c] = val(lam[c]) < 0.0 ? T(0.0) : v[k][c];
+            mat_vec_t(R, rk, u[k]);
+        }
+    } else {
+        return StateT<T>{};
+    }
+    return taylor_rotate_t(u, pr.distance, pr.normal);
+}
+
+// source.rs:7-21 with the exchange coefficients as T
+template <class T> static StateT<T> source_t(const StateT<T>& s, const Params& P, T oei, T oer) {
+    T te = state_te(s, P), tr = state_tr(s, P), ti = state_ti(s, P);
+    return {T(0.0), T(0.0), T(0.0), -oei * (te - ti) - oer * (pow4(te) - pow4(tr)), oei * (te - ti),
+            oer * (pow4(te) - pow4(tr))};
+}
+
+// main.rs:135-305 l() over T at state u (+ tangent), Field::time t
+template <class T>
+static void l_t(const Solver& S, const Tangent& tg, std::vector<StateT<T>>& rhs, std::vector<StateT<T>>& gval) {
+    const Field& f = S.f;
+    const GhostGrid& gg = S.gg;
+    const Params& P = S.P;
+    const long nx = f.grid.nx, ny = f.grid.ny, n = nx * ny;
+    const double dx = f.grid.dx, dy = f.grid.dy;
+    std::vector<StateT<T>> u((size_t)n);
+    for (long l = 0; l < n; ++l)
+        for (int c = 0; c < 6; ++c) u[l][c] = seed<T>(f.value[l][c], tg.du && f.fluid[l] ? tg.du[6 * l + c] : 0.0);
+    gval.assign(gg.info.size(), StateT<T>{});
+    std::vector<DerivedT<T>> gder(gg.info.size()), der((size_t)n);
+    for (size_t g = 0; g < gg.info.size(); ++g) {
+        gval[g] = set_ghost_point_value_t<T>(gg.info[g], f, u.data(), f.time, gg, P, tg);
+        gder[g] = derived_from_state(gval[g], P);
+    }
+    for (long l = 0; l < n; ++l)
+        if (f.fluid[l]) der[l] = derived_from_state(u[l], P);
+    auto v_at = [&](uint32_t t) { return t < (uint32_t)n ? u[t] : gval[t - n]; };
+    auto d_at = [&](uint32_t t) { return t < (uint32_t)n ? der[t] : gder[t - n]; };
+    auto gather6 = [&](size_t anchor, long di0, Dir dir, StateT<T> st[6], DerivedT<T> dd[6]) {
+        for (long q = 0; q < 6; ++q) {
+            long d = di0 + q;
+            int k = dir == DIR_X ? gg.k_for(d, 0) : gg.k_for(0, d);
+            uint32_t t = gg.access[anchor * gg.n_offsets + k];
+            st[q] = v_at(t);
+            dd[q] = d_at(t);
+        }
+    };
+    StateT<T> z{};
+    std::vector<StateT<T>> fx((size_t)(nx + 1) * ny, z), fy((size_t)nx * (ny + 1), z);
+    std::vector<StateT<T>> dfx((size_t)(nx + 1) * ny, z), dfy((size_t)nx * (ny + 1), z);
+    const bool diff = P.diffusion_active();
+    for (long lin = 0; lin < (nx + 1) * ny; ++lin) {
+        long i = lin / ny;
+        size_t anchor; long di0;
+        if (i < nx && f.fluid[lin]) { anchor = lin; di0 = -3; }
+        else if (i >= 1 && f.fluid[lin - ny]) { anchor = lin - ny; di0 = -2; }
+        else continue;
+        StateT<T> st[6]; DerivedT<T> dd[6];
+        gather6(anchor, di0, DIR_X, st, dd);
+        fx[lin] = reconstruction_fast(st, dd, DIR_X, true, P);
+        if (diff) dfx[lin] = diffusion_from_derived(dd, P);
+    }
+    for (long lin = 0; lin < nx * (ny + 1); ++lin) {
+        long j = lin / nx, i = lin % nx;
+        size_t cell = (size_t)i * ny + j;
+        size_t anchor; long di0;
+        if (j < ny && f.fluid[cell]) { anchor = cell; di0 = -3; }
+        else if (j >= 1 && f.fluid[cell - 1]) { anchor = cell - 1; di0 = -2; }
+        else continue;
+        StateT<T> st[6]; DerivedT<T> dd[6];
+        gather6(anchor, di0, DIR_Y, st, dd);
+        fy[lin] = reconstruction_fast(st, dd, DIR_Y, true, P);
+        if (diff) dfy[lin] = diffusion_from_derived(dd, P);
+    }
+    const bool src = P.source_active() || tg.domega_ei != 0.0 || tg.domega_er != 0.0;
+    const T oei = seed<T>(P.omega_ei, tg.domega_ei), oer = seed<T>(P.omega_er, tg.domega_er);
+    rhs.assign((size_t)n, z);
+    for (long lin = 0; lin < n; ++lin) {
+        if (!f.fluid[lin]) continue;
+        long i = lin / ny, j = lin % ny;
+        const StateT<T>& fl = fx[lin];
+        const StateT<T>& fr = fx[lin + ny];
+        const StateT<T>& fb = fy[j * nx + i];
+        const StateT<T>& ft = fy[(j + 1) * nx + i];
+        double sx = 1.0 / dx, sy = 1.0 / dy;
+        StateT<T> fxt, fyt;
+        for (int c = 0; c < 6; ++c) {
+            fxt[c] = -(fr[c] - fl[c]) * sx;
+            fyt[c] = -(ft[c] - fb[c]) * sy;
+        }
+        DerivedT<T> dx9[9], dy9[9];
+        for (long q = 0; q < 9; ++q) {
+            dx9[q] = d_at(gg.access[lin * gg.n_offsets + gg.k_for(-4 + q, 0)]);
+            dy9[q] = d_at(gg.access[lin * gg.n_offsets + gg.k_for(0, -4 + q)]);
+        }
+        StateT<T> ncx = nonconservative_pre(dx9, dx, DIR_X);
+        StateT<T> ncy = nonconservative_pre(dy9, dy, DIR_Y);
+        StateT<T> so = src ? source_t(u[lin], P, oei, oer) : z;
+        StateT<T> dif = z;
+        if (diff) {
+            double cx = -1.0 / (dx * dx), cy = -1.0 / (dy * dy);
+            const StateT<T>& a = dfx[lin];
+            const StateT<T>& b = dfx[lin + ny];
+            const StateT<T>& c2 = dfy[j * nx + i];
+            const StateT<T>& d2 = dfy[(j + 1) * nx + i];
+            for (int c = 0; c < 6; ++c) dif[c] = (-(b[c] - a[c]) * cx) + (-(d2[c] - c2[c]) * cy);
+        }
+        StateT<T> o;
+        for (int c = 0; c < 6; ++c) o[c] = fxt[c] + fyt[c] + ncx[c] + ncy[c] + so[c] + dif[c];
+        rhs[lin] = o;
+    }
+}
+
 } // namespace oracle
 
 // ================================================================ C API
@@ -831,6 +1149,42 @@ int oracle_l(void* h, double* rhs_out, double* ghost_out) {
     } catch (OracleError& e) { set_err((Handle*)h, e); return e.code; }
     if (rhs_out) std::memcpy(rhs_out, s.rhs.data(), s.rhs.size() * sizeof(State));
     if (ghost_out) std::memcpy(ghost_out, s.gg.values.data(), s.gg.values.size() * sizeof(State));
+    return 0;
+}
+
+// J_l(u) du of l() at the current state and time (forward mode, jvp.hpp):
+// rhs/drhs nx*ny*6, ghost/dghost n_ghosts*6 (any may be null); duinf6: the
+// direction of every FarField state; domega2: directions of omega_ei, omega_er.
+int oracle_l_jvp(void* h, const double* du, const double* duinf6, const double* domega2, double* rhs,
+                 double* drhs, double* ghost, double* dghost) {
+    Solver& s = ((Handle*)h)->s;
+    Tangent tg;
+    tg.du = du;
+    if (duinf6) for (int c = 0; c < 6; ++c) tg.duinf[c] = duinf6[c];
+    if (domega2) { tg.domega_ei = domega2[0]; tg.domega_er = domega2[1]; }
+    std::vector<StateT<Dual>> r, g;
+    try { l_t<Dual>(s, tg, r, g); } catch (OracleError& e) { set_err((Handle*)h, e); return e.code; }
+    for (size_t l = 0; l < r.size(); ++l)
+        for (int c = 0; c < 6; ++c) {
+            if (rhs) rhs[6 * l + c] = r[l][c].v;
+            if (drhs) drhs[6 * l + c] = r[l][c].d;
+        }
+    for (size_t q = 0; q < g.size(); ++q)
+        for (int c = 0; c < 6; ++c) {
+            if (ghost) ghost[6 * q + c] = g[q][c].v;
+            if (dghost) dghost[6 * q + c] = g[q][c].d;
+        }
+    return 0;
+}
+
+// double instantiation of the same templates (checks them against oracle_l)
+int oracle_l_t(void* h, double* rhs, double* ghost) {
+    Solver& s = ((Handle*)h)->s;
+    Tangent tg;
+    std::vector<StateT<double>> r, g;
+    try { l_t<double>(s, tg, r, g); } catch (OracleError& e) { set_err((Handle*)h, e); return e.code; }
+    if (rhs) std::memcpy(rhs, r.data(), r.size() * sizeof(State));
+    if (ghost) std::memcpy(ghost, g.data(), g.size() * sizeof(State));
     return 0;
 }
 
