@@ -4,11 +4,12 @@
 //
 // vjp of l at a stage state X (ghost nodes of X set by the forward ghost
 // update) for a cotangent rbar on the fluid cells, accumulated into Ubar:
-//   k_adj_faces  x and y faces: the face flux cotangent from rbar, then the
-//                reverse of weno.rs:685-802 (R g, WENO5 weights, Lax-Friedrichs
-//                split, L projections, the Roe average of points 2 and 3, the
-//                six physical fluxes) and of diffusion.rs:27-50 -> node
-//                cotangents W (fluid and ghost nodes, atomic adds);
+//   k_adj_flux   x and y face tiles: the face flux cotangent from rbar, then
+//                the reverse of weno.rs:685-802 (R g, WENO5 weights,
+//                Lax-Friedrichs split, L projections, the Roe average of
+//                points 2 and 3, the six physical fluxes) and of
+//                diffusion.rs:27-50 -> node cotangents W (fluid and ghost
+//                nodes, atomic adds);
 //   k_adj_cells  fluid cells: reverse of noncon.rs:288-332 (both directions)
 //                and source.rs:7-21 -> W, and the exchange-coefficient
 //                cotangents;
@@ -21,9 +22,10 @@
 //                (ReflectiveWall, ZerothOrder, Periodic) -> Ubar at the source;
 //   k_adj_fluid  Ubar += W on fluid nodes.
 // The eigenvector matrices of a face enter through its five Roe-averaged
-// scalars (u, v, e_e, e_i, e_r); their partial derivatives come from
-// evaluating the same builders (physics.cuh l_row, r_col) over dual numbers
-// with five tangents (dual.cuh). Everything else is differentiated by hand.
+// scalars (u, v, e_e, e_i, e_r). Since L = R^-1, the cotangent of L is
+// turned into one of R (dL = -L dR L) and only R, which is polynomial in
+// u, v and sqrt(cs2), is differentiated; the CFL time step of a cell is
+// differentiated with dual numbers (dual.cuh). The rest is by hand.
 // Kinks follow the values: d|x|/dx = +1 at 0, max/min pass the derivative to
 // the first argument on ties, a FarField row switches on lambda < 0.
 #include <algorithm>
@@ -35,48 +37,30 @@
 
 namespace rh3t {
 
-using D5 = DualN<5>;
 using D8 = DualN<8>;
-
-// Roe state from the five averaged scalars (the rest of roe_average)
-template <class T>
-__device__ __forceinline__ RoeT<T> roe_from_base(T u, T v, T ee, T ei, T er, const DevParams& P) {
-    RoeT<T> q;
-    q.u = u; q.v = v;
-    q.w2 = sqd(u) + sqd(v);
-    q.ee = ee; q.ei = ei; q.er = er;
-    const double GE = P.gamma_e, GI = P.gamma_i, GR = P.gamma_r;
-    const double gi = GI - 1.0, ge = GE - 1.0, gr = GR - 1.0;
-    const double gt = gi + ge + gr;
-    q.cs2 = GE * ge * ee + GI * gi * ei + GR * gr * er;
-    q.cs = sqrt(q.cs2);
-    q.he = 6.0 * gi * gr * (GI * ei - GR * er) + GE * gt * ee * q.w2;
-    q.hi = 6.0 * ge * gr * (GR * er - GE * ee) + GI * gt * ei * q.w2;
-    q.hr = 6.0 * ge * gi * (GE * ee - GI * ei) + GR * gt * er * q.w2;
-    q.b = gt * (36.0 * ge * gi * gr + gt * sqd(q.w2)) * q.cs2;
-    q.den = 12.0 * q.cs2;
-    return q;
-}
+// the adjoint needs derivatives, not the forward's roundings: constant
+// divisions become multiplications by reciprocals
+constexpr double K3 = 1.0 / 3.0, K6 = 1.0 / 6.0;
 
 // ---------------------------------------------------------------- pointwise vjps
 // state.rs:245-276 primitives: cotangents of (u, v, e_e, e_i, e_r, p_e, p_i,
 // p_r) -> state cotangent (added to sb)
 __device__ __forceinline__ void prim_vjp(const double s[6], const DevParams& P, double bu, double bv, double bee,
                                          double bei, double ber, double bpe, double bpi, double bpr, double sb[6]) {
-    const double rho = s[0], u = s[1] / rho, v = s[2] / rho;
+    const double rho = s[0], ir = 1.0 / rho, u = s[1] * ir, v = s[2] * ir;
     const double w2 = u * u + v * v;
     const double ge = P.gamma_e - 1.0, gi = P.gamma_i - 1.0, gr = P.gamma_r - 1.0;
     const double gp = ge * bpe + gi * bpi + gr * bpr;
-    const double bw2 = -(bee + bei + ber) / 6.0 - gp * rho / 6.0;
-    double brho = -(s[3] * bee + s[4] * bei + s[5] * ber) / (rho * rho) - gp * w2 / 6.0;
+    const double bw2 = -(bee + bei + ber) * K6 - gp * rho * K6;
+    double brho = -(s[3] * bee + s[4] * bei + s[5] * ber) * ir * ir - gp * w2 * K6;
     const double bu2 = bu + 2.0 * u * bw2, bv2 = bv + 2.0 * v * bw2;
-    brho -= (bu2 * u + bv2 * v) / rho;
+    brho -= (bu2 * u + bv2 * v) * ir;
     sb[0] += brho;
-    sb[1] += bu2 / rho;
-    sb[2] += bv2 / rho;
-    sb[3] += bee / rho + ge * bpe;
-    sb[4] += bei / rho + gi * bpi;
-    sb[5] += ber / rho + gr * bpr;
+    sb[1] += bu2 * ir;
+    sb[2] += bv2 * ir;
+    sb[3] += bee * ir + ge * bpe;
+    sb[4] += bei * ir + gi * bpi;
+    sb[5] += ber * ir + gr * bpr;
 }
 
 // state.rs:118-135 temperatures: cotangents of (te, ti, tr) -> sb
@@ -131,32 +115,85 @@ __device__ __forceinline__ void weno5_vjp(const double x[5], double eps, double 
     const double t0 = x[0] - 2.0 * x[1] + x[2], r0 = x[0] - 4.0 * x[1] + 3.0 * x[2];
     const double t1 = x[1] - 2.0 * x[2] + x[3], r1 = x[1] - x[3];
     const double t2 = x[2] - 2.0 * x[3] + x[4], r2 = 3.0 * x[2] - 4.0 * x[3] + x[4];
-    const double b0 = 13.0 / 12.0 * t0 * t0 + 0.25 * r0 * r0;
-    const double b1 = 13.0 / 12.0 * t1 * t1 + 0.25 * r1 * r1;
-    const double b2 = 13.0 / 12.0 * t2 * t2 + 0.25 * r2 * r2;
-    const double a0 = 0.1 / sqd(eps + b0), a1 = 0.6 / sqd(eps + b1), a2 = 0.3 / sqd(eps + b2);
-    const double S = a0 + a1 + a2;
-    const double w0 = a0 / S, w1 = a1 / S, w2 = a2 / S;
-    const double p0 = x[0] / 3.0 - 7.0 / 6.0 * x[1] + 11.0 / 6.0 * x[2];
-    const double p1 = -x[1] / 6.0 + 5.0 / 6.0 * x[2] + x[3] / 3.0;
-    const double p2 = x[2] / 3.0 + 5.0 / 6.0 * x[3] - x[4] / 6.0;
+    const double c1312 = 13.0 / 12.0;
+    const double e0 = 1.0 / (eps + (c1312 * t0 * t0 + 0.25 * r0 * r0));
+    const double e1 = 1.0 / (eps + (c1312 * t1 * t1 + 0.25 * r1 * r1));
+    const double e2 = 1.0 / (eps + (c1312 * t2 * t2 + 0.25 * r2 * r2));
+    const double a0 = 0.1 * e0 * e0, a1 = 0.6 * e1 * e1, a2 = 0.3 * e2 * e2;
+    const double iS = 1.0 / (a0 + a1 + a2);
+    const double w0 = a0 * iS, w1 = a1 * iS, w2 = a2 * iS;
+    const double p0 = x[0] * K3 - 7.0 / 6.0 * x[1] + 11.0 / 6.0 * x[2];
+    const double p1 = -x[1] * K6 + 5.0 / 6.0 * x[2] + x[3] * K3;
+    const double p2 = x[2] * K3 + 5.0 / 6.0 * x[3] - x[4] * K6;
     const double pb0 = w0 * gb, pb1 = w1 * gb, pb2 = w2 * gb;
     const double wb0 = p0 * gb, wb1 = p1 * gb, wb2 = p2 * gb;
     const double m = w0 * wb0 + w1 * wb1 + w2 * wb2;
-    const double ab0 = (wb0 - m) / S, ab1 = (wb1 - m) / S, ab2 = (wb2 - m) / S;
-    const double bb0 = -2.0 * ab0 * a0 / (eps + b0), bb1 = -2.0 * ab1 * a1 / (eps + b1),
-                 bb2 = -2.0 * ab2 * a2 / (eps + b2);
-    ub[0] += pb0 / 3.0;
-    ub[1] += -7.0 / 6.0 * pb0 - pb1 / 6.0;
-    ub[2] += 11.0 / 6.0 * pb0 + 5.0 / 6.0 * pb1 + pb2 / 3.0;
-    ub[3] += pb1 / 3.0 + 5.0 / 6.0 * pb2;
-    ub[4] += -pb2 / 6.0;
+    // alpha_k = d_k / (eps + b_k)^2, w_k = alpha_k / sum
+    const double bb0 = -2.0 * (wb0 - m) * iS * a0 * e0, bb1 = -2.0 * (wb1 - m) * iS * a1 * e1,
+                 bb2 = -2.0 * (wb2 - m) * iS * a2 * e2;
+    ub[0] += pb0 * K3;
+    ub[1] += -7.0 / 6.0 * pb0 - pb1 * K6;
+    ub[2] += 11.0 / 6.0 * pb0 + 5.0 / 6.0 * pb1 + pb2 * K3;
+    ub[3] += pb1 * K3 + 5.0 / 6.0 * pb2;
+    ub[4] += -pb2 * K6;
     const double c0 = 13.0 / 6.0 * t0 * bb0, d0 = 0.5 * r0 * bb0;
     ub[0] += c0 + d0; ub[1] += -2.0 * c0 - 4.0 * d0; ub[2] += c0 + 3.0 * d0;
     const double c1 = 13.0 / 6.0 * t1 * bb1, d1 = 0.5 * r1 * bb1;
     ub[1] += c1 + d1; ub[2] += -2.0 * c1; ub[3] += c1 - d1;
     const double c2 = 13.0 / 6.0 * t2 * bb2, d2 = 0.5 * r2 * bb2;
     ub[2] += c2 + 3.0 * d2; ub[3] += -2.0 * c2 - 4.0 * d2; ub[4] += c2 + d2;
+}
+
+// weno5 of the forward written with reciprocals (the adjoint's recomputation)
+__device__ __forceinline__ double weno5_adj(const double x[5], double eps) {
+    const double c1312 = 13.0 / 12.0;
+    const double t0 = x[0] - 2.0 * x[1] + x[2], r0 = x[0] - 4.0 * x[1] + 3.0 * x[2];
+    const double t1 = x[1] - 2.0 * x[2] + x[3], r1 = x[1] - x[3];
+    const double t2 = x[2] - 2.0 * x[3] + x[4], r2 = 3.0 * x[2] - 4.0 * x[3] + x[4];
+    const double e0 = 1.0 / (eps + (c1312 * t0 * t0 + 0.25 * r0 * r0));
+    const double e1 = 1.0 / (eps + (c1312 * t1 * t1 + 0.25 * r1 * r1));
+    const double e2 = 1.0 / (eps + (c1312 * t2 * t2 + 0.25 * r2 * r2));
+    const double a0 = 0.1 * e0 * e0, a1 = 0.6 * e1 * e1, a2 = 0.3 * e2 * e2;
+    const double p0 = x[0] * K3 - 7.0 / 6.0 * x[1] + 11.0 / 6.0 * x[2];
+    const double p1 = -x[1] * K6 + 5.0 / 6.0 * x[2] + x[3] * K3;
+    const double p2 = x[2] * K3 + 5.0 / 6.0 * x[3] - x[4] * K6;
+    return (a0 * p0 + a1 * p1 + a2 * p2) / (a0 + a1 + a2);
+}
+
+// column c of R and lambda_c (weno.rs:518-545) with reciprocals
+template <int DIR>
+__device__ __forceinline__ void r_col_adj(int c, const Roe& q, const DevParams& P, double R[6], double& lam) {
+    const double GE = P.gamma_e, GI = P.gamma_i, GR = P.gamma_r;
+    const double gi = GI - 1.0, ge = GE - 1.0, gr = GR - 1.0;
+    const double gt = gi + ge + gr;
+    const double u = q.u, v = q.v, w2 = q.w2, cs = q.cs, vel = DIR == 0 ? u : v;
+    const double w6 = w2 * K6;
+    if (c == 0 || c == 5) {
+        const double sg = c == 0 ? -1.0 : 1.0, vc = sg * vel * cs * K3;
+        R[0] = 1.0;
+        R[1] = DIR == 0 ? u + sg * cs : u;
+        R[2] = DIR == 0 ? v : v + sg * cs;
+        R[3] = GE * q.ee + w6 + vc; R[4] = GI * q.ei + w6 + vc; R[5] = GR * q.er + w6 + vc;
+        lam = vel + sg * cs;
+        return;
+    }
+    lam = vel;
+    const int tr = DIR == 0 ? 4 : 1; // transverse column
+    if (c == tr) {
+        const double t3 = (DIR == 0 ? v : u) * K3;
+        R[0] = 0.0;
+        R[1] = DIR == 0 ? 0.0 : 1.0;
+        R[2] = DIR == 0 ? 1.0 : 0.0;
+        R[3] = t3; R[4] = t3; R[5] = t3;
+        return;
+    }
+    const int k = DIR == 0 ? c - 1 : c - 2; // species 0 e, 1 i, 2 r
+    const double gk = k == 0 ? ge : (k == 1 ? gi : gr);
+    const double sp = gt * w2 * K6 / gk;
+    R[0] = 1.0; R[1] = u; R[2] = v;
+    if (k == 0) { R[3] = sp; R[4] = gr; R[5] = -gi; }
+    else if (k == 1) { R[3] = -gr; R[4] = sp; R[5] = ge; }
+    else { R[3] = gi; R[4] = -ge; R[5] = sp; }
 }
 
 // Roe base cotangents (u, v, e_e, e_i, e_r) -> state cotangents of the two
@@ -180,22 +217,80 @@ __device__ __forceinline__ void roe_vjp(const double sa[6], const double sb_[6],
     prim_vjp(sb_, P, pb[0], pb[1], pb[2], pb[3], pb[4], 0.0, 0.0, 0.0, gb);
 }
 
-// Roe base cotangent of (L row c, R column c, lambda_c) cotangents
+// Cotangents of R (Rb[c][i] = dJ/dR[i][c], weno.rs:518-545) and of the
+// eigenvalues -> cotangents of the Roe base (u, v, e_e, e_i, e_r), added.
+// R is written in u, v, w2 = u^2 + v^2, cs = sqrt(cs2) and the e_k.
 template <int DIR>
-__device__ __forceinline__ void lr_base_vjp(int c, const double base[5], const DevParams& P, const double Lb[6],
-                                            const double Rb[6], double lamb, double bb[5]) {
-    const RoeT<D5> q = roe_from_base(D5::var(base[0], 0), D5::var(base[1], 1), D5::var(base[2], 2),
-                                     D5::var(base[3], 3), D5::var(base[4], 4), P);
-    D5 L[6], R[6], lam;
-    l_row<DIR>(c, q, P, L);
-    r_col<DIR>(c, q, P, R, lam);
-#pragma unroll
-    for (int m = 0; m < 5; ++m) {
-        double acc = lamb * lam.d[m];
-#pragma unroll
-        for (int j = 0; j < 6; ++j) acc += Lb[j] * L[j].d[m] + Rb[j] * R[j].d[m];
-        bb[m] += acc;
+__device__ __forceinline__ void r_base_vjp(const double base[5], const DevParams& P, const double Rb[6][6],
+                                           const double lamb[6], double bb[5]) {
+    const double GE = P.gamma_e, GI = P.gamma_i, GR = P.gamma_r;
+    const double gi = GI - 1.0, ge = GE - 1.0, gr = GR - 1.0;
+    const double gt = gi + ge + gr;
+    const double u = base[0], v = base[1];
+    const double cs = sqrt(GE * ge * base[2] + GI * gi * base[3] + GR * gr * base[4]);
+    const double vel = DIR == 0 ? u : v;
+    double bvel = 0.0, bcs = 0.0, bw2 = 0.0, bu = 0.0, bv = 0.0, be[3] = {0.0, 0.0, 0.0};
+    const double Gk[3] = {GE, GI, GR}, gk[3] = {ge, gi, gr};
+    // acoustic columns 0 (-) and 5 (+): (1, [vel -+ cs], ..., G_k e_k + w2/6 -+ vel cs/3)
+    for (int side = 0; side < 2; ++side) {
+        const int c = side == 0 ? 0 : 5;
+        const double sg = side == 0 ? -1.0 : 1.0;
+        const double* r = Rb[c];
+        if (DIR == 0) { bu += r[1]; bcs += sg * r[1]; bv += r[2]; }
+        else { bu += r[1]; bv += r[2]; bcs += sg * r[2]; }
+        for (int k = 0; k < 3; ++k) {
+            be[k] += Gk[k] * r[3 + k];
+            bw2 += r[3 + k] * K6;
+            bvel += sg * cs * K3 * r[3 + k];
+            bcs += sg * vel * K3 * r[3 + k];
+        }
     }
+    // transverse column (x: 4, y: 1): unit momentum, (t/3, t/3, t/3) with t = v (x) or u (y)
+    {
+        const int c = DIR == 0 ? 4 : 1;
+        const double t3 = (Rb[c][3] + Rb[c][4] + Rb[c][5]) * K3;
+        if (DIR == 0) bv += t3;
+        else bu += t3;
+    }
+    // species columns (x: 1, 2, 3; y: 2, 3, 4): (1, u, v, ..., gt w2 / (6 g_k) at row 3 + k)
+    for (int k = 0; k < 3; ++k) {
+        const int c = DIR == 0 ? 1 + k : 2 + k;
+        bu += Rb[c][1];
+        bv += Rb[c][2];
+        bw2 += gt * K6 / gk[k] * Rb[c][3 + k];
+    }
+    // eigenvalues: vel -+ cs, vel
+    for (int c = 0; c < 6; ++c) bvel += lamb[c];
+    bcs += lamb[5] - lamb[0];
+    if (DIR == 0) bu += bvel;
+    else bv += bvel;
+    bu += 2.0 * u * bw2;
+    bv += 2.0 * v * bw2;
+    const double hc = 0.5 / cs;
+    bb[0] += bu;
+    bb[1] += bv;
+    bb[2] += be[0] + GE * ge * hc * bcs;
+    bb[3] += be[1] + GI * gi * hc * bcs;
+    bb[4] += be[2] + GR * gr * hc * bcs;
+}
+
+// L = R^-1, so dL = -L dR L and the cotangent Lb of L is one of R:
+// Rb -= L^T Lb L^T. Rb[c][i] = dJ/dR[i][c], Lb[c][j] = dJ/dL[c][j],
+// L[c][j] = L[6c + j].
+__device__ __forceinline__ void fold_l_into_r(const double* L, const double Lb[6][6], double Rb[6][6]) {
+    double Z[6][6]; // Z[j][c] = sum_k Lb[j][k] L[c][k]
+    for (int j = 0; j < 6; ++j)
+        for (int c = 0; c < 6; ++c) {
+            double acc = 0.0;
+            for (int k = 0; k < 6; ++k) acc += Lb[j][k] * L[6 * c + k];
+            Z[j][c] = acc;
+        }
+    for (int c = 0; c < 6; ++c)
+        for (int i = 0; i < 6; ++i) {
+            double acc = 0.0;
+            for (int j = 0; j < 6; ++j) acc += L[6 * j + i] * Z[j][c];
+            Rb[c][i] -= acc;
+        }
 }
 
 __device__ __forceinline__ void atomic_add6(double* W, long long plane, long long n, const double v[6]) {
@@ -204,82 +299,143 @@ __device__ __forceinline__ void atomic_add6(double* W, long long plane, long lon
         if (v[c] != 0.0) atomicAdd(&W[c * plane + n], v[c]);
 }
 
-// ---------------------------------------------------------------- faces
-// rbar: cell cotangent planes (padded, zero off the fluid); W: node cotangents
+// ---------------------------------------------------------------- face tiles
+// The same 64-face tiles as the forward flux kernel (k_flux), block of 6
+// warps:
+//   1. staging: point states and physical fluxes of the tile, each face's Roe
+//      state and flux cotangent Fb (from rbar);
+//   2. warp c = characteristic field c, faces lane and lane + 32: the forward
+//      reconstruction of field c, then its reverse: w-bar and f-bar of the six
+//      points, L-bar of row c, lambda-bar; L row c and g_c kept for step 3;
+//   3a. three threads per face: L-bar folded into R-bar (L = R^-1), the Roe
+//      base cotangent and the Roe average's vjp -> W at points 2 and 3
+//      (atomic), the diffusion flux's vjp, and per point k of the face
+//      sum_c w-bar_ck L_c and sum_c f-bar_ck L_c;
+//   3b. one thread per point: the sums of 3a over the faces that use it, the
+//      physical flux's vjp -> W (atomic).
+struct AdjFluxShared {
+    double2 U[3][FLUX_NPT];
+    double2 F[3][FLUX_NPT];
+    double Q[15][FLUX_FACES];     // Roe state u v w2 ee ei er cs2 cs he hi hr b den, 1/cs2, 1/b
+    double FB[6][FLUX_FACES];     // face flux cotangent
+    double G[6][FLUX_FACES];      // g_c
+    double LAMB[6][FLUX_FACES];   // lambda-bar_c
+    double LS[6][6][FLUX_FACES];  // L row c
+    double LB[6][6][FLUX_FACES];  // L-bar row c
+    double WB[6][6][FLUX_FACES];  // w-bar [c][k]
+    double FK[6][6][FLUX_FACES];  // f-bar [c][k]
+    int act[FLUX_FACES];
+};
+
 template <int DIR>
-__device__ void face_vjp(const Inst& I, const double* __restrict__ X, const double* __restrict__ rbar,
-                         double* __restrict__ W, int i, int j) {
+__device__ __forceinline__ void adj_face_index(const Tile& t, int f, int& i, int& j, int& p0, int& ps) {
+    const int r = f >> t.lg, cc = f & ((1 << t.lg) - 1);
+    i = t.i + r;
+    j = t.j0 + cc;
+    if (DIR == 0) { p0 = f; ps = 1 << t.lg; }
+    else { p0 = r * ((1 << t.lg) + 5) + cc; ps = 1; }
+}
+
+__device__ __forceinline__ Roe adj_load_q(const AdjFluxShared& S, int f) {
+    Roe q;
+    q.u = S.Q[0][f]; q.v = S.Q[1][f]; q.w2 = S.Q[2][f]; q.ee = S.Q[3][f]; q.ei = S.Q[4][f]; q.er = S.Q[5][f];
+    q.cs2 = S.Q[6][f]; q.cs = S.Q[7][f]; q.he = S.Q[8][f]; q.hi = S.Q[9][f]; q.hr = S.Q[10][f]; q.b = S.Q[11][f];
+    q.den = S.Q[12][f];
+    return q;
+}
+
+__device__ __forceinline__ void adj_point(const AdjFluxShared& S, int p, double u[6], double F[6]) {
+    const double2 a = S.U[0][p], b = S.U[1][p], c = S.U[2][p];
+    const double2 x = S.F[0][p], y = S.F[1][p], z = S.F[2][p];
+    u[0] = a.x; u[1] = a.y; u[2] = b.x; u[3] = b.y; u[4] = c.x; u[5] = c.y;
+    F[0] = x.x; F[1] = x.y; F[2] = y.x; F[3] = y.y; F[4] = z.x; F[5] = z.y;
+}
+
+template <int DIR>
+__device__ void adj_flux_tile(const Inst& I, const Tile& t, const double* __restrict__ X,
+                              const double* __restrict__ rbar, double* __restrict__ W, AdjFluxShared& S) {
     const DevParams& P = I.P;
     const long long plane = I.plane;
     const int nx = I.nx, ny = I.ny;
-    // activity (main.rs:165-246): a face with a fluid cell on either side
-    const long long n3 = node_of(I, i, j), n2 = DIR == 0 ? node_of(I, i - 1, j) : node_of(I, i, j - 1);
-    if (!(I.mask[n3] | I.mask[n2])) return;
+    const int cols = 1 << t.lg, rows = FLUX_FACES >> t.lg;
+    const int np = DIR == 0 ? (rows + 5) * cols : rows * (cols + 5);
     const double sc = DIR == 0 ? 1.0 / I.dx : 1.0 / I.dy;
-    double Fb[6];
-    const bool in3 = DIR == 0 ? (i < nx) : (j < ny);
-    const bool in2 = DIR == 0 ? (i >= 1) : (j >= 1);
-#pragma unroll
-    for (int c = 0; c < 6; ++c) {
-        const double r3 = in3 && I.mask[n3] ? rbar[c * plane + n3] : 0.0;
-        const double r2 = in2 && I.mask[n2] ? rbar[c * plane + n2] : 0.0;
-        Fb[c] = (r3 - r2) * sc;
-    }
-    // stencil points i-3..i+2 (x) / j-3..j+2 (y)
-    double s[6][6];
-    long long nd[6];
-#pragma unroll
-    for (int k = 0; k < 6; ++k) {
-        nd[k] = DIR == 0 ? node_of(I, i - 3 + k, j) : node_of(I, i, j - 3 + k);
-        load6(X, plane, nd[k], s[k]);
-    }
-    Prim d[6];
-    double F[6][6];
-#pragma unroll
-    for (int k = 0; k < 6; ++k) {
-        d[k] = prim_from_state(s[k], P);
-        phys_flux<DIR>(s[k], d[k], F[k]);
-    }
-    const Roe q = roe_average(s[3][0], d[3], s[2][0], d[2], P);
-    const double base[5] = {q.u, q.v, q.ee, q.ei, q.er};
-    double sbar[6][6], Fbar[6][6], bb[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-    for (int k = 0; k < 6; ++k)
-#pragma unroll
-        for (int m = 0; m < 6; ++m) { sbar[k][m] = 0.0; Fbar[k][m] = 0.0; }
-    // g_c for R-bar needs all six reconstructions first
-    double g[6];
-    for (int c = 0; c < 6; ++c) {
-        double Lc[6];
-        l_row<DIR>(c, q, P, Lc);
-        const double vel = DIR == 0 ? q.u : q.v;
-        const double lam = c == 0 ? vel - q.cs : (c == 5 ? vel + q.cs : vel);
-        const double a = fabs(lam);
-        double fp[6], fm[6];
-        for (int k = 0; k < 6; ++k) {
-            double cf = 0.0, cs = 0.0;
-            for (int m = 0; m < 6; ++m) { cf += Lc[m] * F[k][m]; cs += Lc[m] * s[k][m]; }
-            fp[k] = 0.5 * (cf + a * cs);
-            fm[k] = 0.5 * (cf - a * cs);
+    // ---- 1. staging
+    for (int w = threadIdx.x; w < np + FLUX_FACES; w += blockDim.x) {
+        if (w < np) {
+            const int p = w;
+            int pi, pj;
+            if (DIR == 0) { pi = t.i - 3 + (p >> t.lg); pj = t.j0 + (p & (cols - 1)); }
+            else { const int r = p / (cols + 5); pi = t.i + r; pj = t.j0 - 3 + (p - r * (cols + 5)); }
+            double s[6] = {1.0, 0.0, 0.0, 1.0, 1.0, 1.0};
+            if (pi >= -RH3T_PAD && pi < nx + RH3T_PAD && pj >= -RH3T_PAD && pj < ny + RH3T_PAD)
+                load6(X, plane, node_of(I, pi, pj), s);
+            const Prim d = prim_from_state(s, P);
+            double f[6];
+            phys_flux<DIR>(s, d, f);
+            for (int k = 0; k < 3; ++k) {
+                S.U[k][p] = make_double2(s[2 * k], s[2 * k + 1]);
+                S.F[k][p] = make_double2(f[2 * k], f[2 * k + 1]);
+            }
+        } else {
+            const int f = w - np;
+            int i, j, p0, ps;
+            adj_face_index<DIR>(t, f, i, j, p0, ps);
+            bool valid = DIR == 0 ? (i <= nx && j < ny) : (i < nx && j <= ny);
+            long long n3 = 0, n2 = 0;
+            if (valid) {
+                n3 = node_of(I, i, j);
+                n2 = DIR == 0 ? node_of(I, i - 1, j) : node_of(I, i, j - 1);
+                valid = (I.mask[n3] | I.mask[n2]) != 0;
+            }
+            S.act[f] = valid ? 1 : 0;
+            if (!valid) continue;
+            double s3[6], s2[6];
+            load6(X, plane, n3, s3);
+            load6(X, plane, n2, s2);
+            const Prim d3 = prim_from_state(s3, P), d2 = prim_from_state(s2, P);
+            const Roe q = roe_average(s3[0], d3, s2[0], d2, P);
+            const double qv[15] = {q.u,  q.v,  q.w2, q.ee, q.ei, q.er,  q.cs2,       q.cs,
+                                   q.he, q.hi, q.hr, q.b,  q.den, 1.0 / q.cs2, 1.0 / q.b};
+            for (int k = 0; k < 15; ++k) S.Q[k][f] = qv[k];
+            const bool in3 = DIR == 0 ? (i < nx) : (j < ny);
+            const bool in2 = DIR == 0 ? (i >= 1) : (j >= 1);
+            for (int c = 0; c < 6; ++c) {
+                const double r3 = in3 && I.mask[n3] ? rbar[c * plane + n3] : 0.0;
+                const double r2 = in2 && I.mask[n2] ? rbar[c * plane + n2] : 0.0;
+                S.FB[c][f] = (r3 - r2) * sc;
+            }
         }
-        g[c] = weno5(fp[0], fp[1], fp[2], fp[3], fp[4], P.eps) + weno5(fm[5], fm[4], fm[3], fm[2], fm[1], P.eps);
     }
-    for (int c = 0; c < 6; ++c) {
+    __syncthreads();
+    // ---- 2. warp c: field c of faces lane and lane + 32
+    const int c = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int h = 0; h < FLUX_FACES / 32; ++h) {
+        const int f = lane + 32 * h;
+        if (!S.act[f]) continue;
+        int i, j, p0, ps;
+        adj_face_index<DIR>(t, f, i, j, p0, ps);
+        const Roe q = adj_load_q(S, f);
         double Lc[6], Rc[6], lam;
-        l_row<DIR>(c, q, P, Lc);
-        r_col<DIR>(c, q, P, Rc, lam);
-        // F_i = sum_c R_ic g_c
-        double gb = 0.0, Rb[6];
-        for (int i2 = 0; i2 < 6; ++i2) { gb += Rc[i2] * Fb[i2]; Rb[i2] = Fb[i2] * g[c]; }
+        fastm::l_row<DIR>(c, q, S.Q[13][f], S.Q[14][f], P, Lc);
+        r_col_adj<DIR>(c, q, P, Rc, lam);
         const double a = fabs(lam);
-        double w[6], f[6], fp[6], fm[6];
+        double w[6], fp[6], fm[6];
         for (int k = 0; k < 6; ++k) {
+            double u[6], F[6];
+            adj_point(S, p0 + k * ps, u, F);
             double cf = 0.0, cs = 0.0;
-            for (int m = 0; m < 6; ++m) { cf += Lc[m] * F[k][m]; cs += Lc[m] * s[k][m]; }
-            f[k] = cf; w[k] = cs;
+            for (int m = 0; m < 6; ++m) { cf += Lc[m] * F[m]; cs += Lc[m] * u[m]; }
+            w[k] = cs;
             fp[k] = 0.5 * (cf + a * cs);
             fm[k] = 0.5 * (cf - a * cs);
         }
+        {
+            const double xm[5] = {fm[5], fm[4], fm[3], fm[2], fm[1]};
+            S.G[c][f] = weno5_adj(fp, P.eps) + weno5_adj(xm, P.eps);
+        }
+        double gb = 0.0;
+        for (int i2 = 0; i2 < 6; ++i2) gb += Rc[i2] * S.FB[i2][f];
         double fpb[6] = {0, 0, 0, 0, 0, 0}, fmb[6] = {0, 0, 0, 0, 0, 0};
         weno5_vjp(fp, P.eps, gb, fpb);
         {
@@ -293,59 +449,159 @@ __device__ void face_vjp(const Inst& I, const double* __restrict__ X, const doub
             const double fbk = 0.5 * (fpb[k] + fmb[k]);
             const double wbk = 0.5 * a * (fpb[k] - fmb[k]);
             ab += 0.5 * w[k] * (fpb[k] - fmb[k]);
-            for (int m = 0; m < 6; ++m) {
-                Lb[m] += wbk * s[k][m] + fbk * F[k][m];
-                sbar[k][m] += wbk * Lc[m];
-                Fbar[k][m] += fbk * Lc[m];
+            double u[6], F[6];
+            adj_point(S, p0 + k * ps, u, F);
+            for (int m = 0; m < 6; ++m) Lb[m] += wbk * u[m] + fbk * F[m];
+            S.WB[c][k][f] = wbk;
+            S.FK[c][k][f] = fbk;
+        }
+        for (int m = 0; m < 6; ++m) { S.LS[c][m][f] = Lc[m]; S.LB[c][m][f] = Lb[m]; }
+        S.LAMB[c][f] = lam < 0.0 ? -ab : ab;
+    }
+    __syncthreads();
+    // ---- 3a. per face, three threads (two columns of R each): L-bar folded
+    // into R-bar (L = R^-1), the Roe base cotangent; then the Roe average's
+    // vjp and the diffusion flux's vjp on the first of the three
+    {
+        const int f = threadIdx.x / 3, part = threadIdx.x - 3 * (threadIdx.x / 3);
+        const bool on = f < FLUX_FACES && S.act[f];
+        double bb[5] = {0, 0, 0, 0, 0};
+        if (on) {
+            double Rb[6][6], lamb[6];
+            for (int c2 = 0; c2 < 6; ++c2) {
+                const bool mine = (c2 >> 1) == part;
+                lamb[c2] = mine ? S.LAMB[c2][f] : 0.0;
+                for (int m = 0; m < 6; ++m) Rb[c2][m] = mine ? S.FB[m][f] * S.G[c2][f] : 0.0;
+            }
+            // Rb[c][i] -= sum_j L[j][i] Z[j][c], Z[j][c] = sum_k Lb[j][k] L[c][k], own columns c
+            for (int c2 = 2 * part; c2 < 2 * part + 2; ++c2) {
+                double Z[6];
+                for (int j = 0; j < 6; ++j) {
+                    double acc = 0.0;
+                    for (int k = 0; k < 6; ++k) acc += S.LB[j][k][f] * S.LS[c2][k][f];
+                    Z[j] = acc;
+                }
+                for (int i = 0; i < 6; ++i) {
+                    double acc = 0.0;
+                    for (int j = 0; j < 6; ++j) acc += S.LS[j][i][f] * Z[j];
+                    Rb[c2][i] -= acc;
+                }
+            }
+            const Roe q = adj_load_q(S, f);
+            const double base[5] = {q.u, q.v, q.ee, q.ei, q.er};
+            r_base_vjp<DIR>(base, P, Rb, lamb, bb);
+        }
+        // per face and point k of this part: V_k = sum_c wbar_ck L_c and
+        // VF_k = sum_c fbar_ck L_c (the point sums of 3b read these)
+        double V[2][6], VF[2][6];
+        if (on)
+            for (int h = 0; h < 2; ++h) {
+                const int k = 2 * part + h;
+                for (int m = 0; m < 6; ++m) {
+                    double a = 0.0, b = 0.0;
+                    for (int c2 = 0; c2 < 6; ++c2) {
+                        const double l = S.LS[c2][m][f];
+                        a += S.WB[c2][k][f] * l;
+                        b += S.FK[c2][k][f] * l;
+                    }
+                    V[h][m] = a;
+                    VF[h][m] = b;
+                }
+            }
+        __syncthreads(); // LB, WB, G and LAMB are read: reuse them
+        if (on) {
+            if (part == 1) for (int m = 0; m < 5; ++m) S.G[m][f] = bb[m];
+            if (part == 2) for (int m = 0; m < 5; ++m) S.LAMB[m][f] = bb[m];
+            for (int h = 0; h < 2; ++h)
+                for (int m = 0; m < 6; ++m) {
+                    S.LB[2 * part + h][m][f] = V[h][m];
+                    S.WB[2 * part + h][m][f] = VF[h][m];
+                }
+        }
+        __syncthreads();
+        if (on && part == 0) {
+            for (int m = 0; m < 5; ++m) bb[m] += S.G[m][f] + S.LAMB[m][f];
+            int i, j, p0, ps;
+            adj_face_index<DIR>(t, f, i, j, p0, ps);
+            double u3[6], u2[6], F_[6];
+            adj_point(S, p0 + 3 * ps, u3, F_);
+            adj_point(S, p0 + 2 * ps, u2, F_);
+            double g3[6] = {0, 0, 0, 0, 0, 0}, g2[6] = {0, 0, 0, 0, 0, 0};
+            roe_vjp(u3, u2, P, bb, g3, g2);
+            atomic_add6(W, plane, node_of(I, i, j), g3);
+            atomic_add6(W, plane, DIR == 0 ? node_of(I, i - 1, j) : node_of(I, i, j - 1), g2);
+            if (I.diffusion) { // diffusion.rs:27-50: rhs += -(b - a) cx per face pair, cx = -1 / ds^2
+                const double cx = DIR == 0 ? -1.0 / (I.dx * I.dx) : -1.0 / (I.dy * I.dy);
+                const double Db[3] = {S.FB[3][f] / sc * cx, S.FB[4][f] / sc * cx, S.FB[5][f] / sc * cx};
+                const double cf[6] = {-2.0, 25.0, -245.0, 245.0, -25.0, 2.0};
+                const double kap[3] = {P.kappa_e, P.kappa_i, P.kappa_r};
+                for (int k = 0; k < 6; ++k) {
+                    double uk[6];
+                    adj_point(S, p0 + k * ps, uk, F_);
+                    double te, ti, tr;
+                    temps_from_state(uk, P, te, ti, tr);
+                    double sb[6] = {0, 0, 0, 0, 0, 0};
+                    temps_vjp(uk, P, Db[0] * kap[0] * cf[k] / 180.0, Db[1] * kap[1] * cf[k] / 180.0,
+                              Db[2] * kap[2] * cf[k] / 180.0 * 4.0 * tr * tr * tr, sb);
+                    const long long nk = DIR == 0 ? node_of(I, i - 3 + k, j) : node_of(I, i, j - 3 + k);
+                    atomic_add6(W, plane, nk, sb);
+                }
             }
         }
-        const double lamb = lam < 0.0 ? -ab : ab;
-        lr_base_vjp<DIR>(c, base, P, Lb, Rb, lamb, bb);
     }
-    // Roe average of points 3 and 2
-    roe_vjp(s[3], s[2], P, bb, sbar[3], sbar[2]);
-    // physical fluxes
-#pragma unroll
-    for (int k = 0; k < 6; ++k) flux_vjp<DIR>(s[k], d[k], P, Fbar[k], sbar[k]);
-    // diffusion.rs:27-50: rhs += -(b - a) cx per face pair, cx = -1 / ds^2
-    if (I.diffusion) {
-        const double cx = DIR == 0 ? -1.0 / (I.dx * I.dx) : -1.0 / (I.dy * I.dy);
-        double Db[3];
-        for (int m3 = 0; m3 < 3; ++m3) {
-            const double r3 = in3 && I.mask[n3] ? rbar[(3 + m3) * plane + n3] : 0.0;
-            const double r2 = in2 && I.mask[n2] ? rbar[(3 + m3) * plane + n2] : 0.0;
-            Db[m3] = (r3 - r2) * cx;
-        }
-        const double cf[6] = {-2.0, 25.0, -245.0, 245.0, -25.0, 2.0};
-        const double kap[3] = {P.kappa_e, P.kappa_i, P.kappa_r};
+    // ---- 3b. per point: sum over the faces and fields that use it
+    for (int p = threadIdx.x; p < np; p += blockDim.x) {
+        // faces of this point: x tiles: same column, rows pr-5..pr; y tiles: same row, cols pc-5..pc
+        int pr, pc, pi, pj;
+        if (DIR == 0) { pr = p >> t.lg; pc = p & (cols - 1); pi = t.i - 3 + pr; pj = t.j0 + pc; }
+        else { pr = p / (cols + 5); pc = p - pr * (cols + 5); pi = t.i + pr; pj = t.j0 - 3 + pc; }
+        double ub[6] = {0, 0, 0, 0, 0, 0}, fb[6] = {0, 0, 0, 0, 0, 0};
+        bool any = false;
         for (int k = 0; k < 6; ++k) {
-            double te, ti, tr;
-            temps_from_state(s[k], P, te, ti, tr);
-            const double bte = Db[0] * kap[0] * cf[k] / 180.0;
-            const double bti = Db[1] * kap[1] * cf[k] / 180.0;
-            const double btr = Db[2] * kap[2] * cf[k] / 180.0 * 4.0 * tr * tr * tr;
-            temps_vjp(s[k], P, bte, bti, btr, sbar[k]);
+            int f;
+            if (DIR == 0) {
+                const int r = pr - k;
+                if (r < 0 || r >= rows) continue;
+                f = r * cols + pc;
+            } else {
+                const int cc = pc - k;
+                if (cc < 0 || cc >= cols) continue;
+                f = pr * cols + cc;
+            }
+            if (!S.act[f]) continue;
+            any = true;
+            for (int m = 0; m < 6; ++m) {
+                ub[m] += S.LB[k][m][f]; // V_k of face f
+                fb[m] += S.WB[k][m][f]; // VF_k
+            }
         }
+        if (!any) continue;
+        double u[6], F_[6];
+        adj_point(S, p, u, F_);
+        const Prim d = prim_from_state(u, P);
+        flux_vjp<DIR>(u, d, P, fb, ub);
+        atomic_add6(W, plane, node_of(I, pi, pj), ub);
     }
-#pragma unroll
-    for (int k = 0; k < 6; ++k) atomic_add6(W, plane, nd[k], sbar[k]);
 }
 
-// X, rbar, W: batch-wide plane sets (instance k's 6 padded planes at I.aoff)
-__global__ void __launch_bounds__(128) k_adj_faces(const Inst* __restrict__ insts, int k0,
-                                                   const double* __restrict__ X, const double* __restrict__ rbar,
-                                                   double* __restrict__ W, int dir) {
-    const Inst& I = insts[k0 + blockIdx.y];
-    if (has_error(I)) return;
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (dir == 0) {
-        if (t >= (long long)(I.nx + 1) * I.ny) return;
-        const int i = (int)(t / I.ny), j = (int)(t % I.ny);
-        face_vjp<0>(I, X + I.aoff, rbar + I.aoff, W + I.aoff, i, j);
-    } else {
-        if (t >= (long long)I.nx * (I.ny + 1)) return;
-        const int i = (int)(t / (I.ny + 1)), j = (int)(t % (I.ny + 1));
-        face_vjp<1>(I, X + I.aoff, rbar + I.aoff, W + I.aoff, i, j);
+__global__ void __launch_bounds__(FLUX_THREADS, 2) k_adj_flux(const Inst* __restrict__ insts,
+                                                           const Tile* __restrict__ tx, int ntx,
+                                                           const Tile* __restrict__ ty, int nty,
+                                                           const double* __restrict__ Xb,
+                                                           const double* __restrict__ rbarb, double* __restrict__ Wb) {
+    extern __shared__ __align__(16) unsigned char adj_flux_smem[];
+    AdjFluxShared& S = *reinterpret_cast<AdjFluxShared*>(adj_flux_smem);
+    const int b = blockIdx.x;
+    if (b < ntx) {
+        const Tile t = tx[b];
+        const Inst& I = insts[t.inst];
+        if (has_error(I)) return;
+        adj_flux_tile<0>(I, t, Xb + I.aoff, rbarb + I.aoff, Wb + I.aoff, S);
+    } else if (b < ntx + nty) {
+        const Tile t = ty[b - ntx];
+        const Inst& I = insts[t.inst];
+        if (has_error(I)) return;
+        adj_flux_tile<1>(I, t, Xb + I.aoff, rbarb + I.aoff, Wb + I.aoff, S);
     }
 }
 
@@ -419,58 +675,119 @@ __device__ __forceinline__ void noncon9_vjp(const double pe[9], const double pi[
     }
 }
 
-// pbar: per-instance parameter cotangents [u_inf (6), omega_ei, omega_er]
-__global__ void __launch_bounds__(128) k_adj_cells(const Inst* __restrict__ insts, int k0,
-                                                   const double* __restrict__ Xb, const double* __restrict__ rbarb,
-                                                   double* __restrict__ Wb, double* __restrict__ pbar) {
-    const int kk = k0 + blockIdx.y;
-    const Inst& I = insts[kk];
+// Fluid cells on the RHS tiles (a TI x TJ block of cells with its 4-node cross
+// halo, shape per tile): the node primitives (p_e, p_i, p_r, u, v) of the
+// tile and halo are formed once in shared memory; each cell adds the
+// cotangents of its two 9-point stencils to a shared tile of primitive
+// cotangents; each node then turns them into a state cotangent with one
+// primitive vjp and one atomic add per component to W. The exchange source
+// goes to W at the cell, its coefficient cotangents to pbar (block sums).
+// pbar: per-instance parameter cotangents [u_inf (6), omega_ei, omega_er].
+constexpr int ADJ_CELL_SMEM = 2 * 5 * RHS_NPT * (int)sizeof(double);
+
+__global__ void __launch_bounds__(RHS_THREADS) k_adj_cells(const Inst* __restrict__ insts,
+                                                           const Tile* __restrict__ tiles, int nt,
+                                                           const double* __restrict__ Xb,
+                                                           const double* __restrict__ rbarb, double* __restrict__ Wb,
+                                                           double* __restrict__ pbar) {
+    extern __shared__ __align__(16) double adj_cell_smem[];
+    double* sP = adj_cell_smem;                // [5][RHS_NPT] p_e, p_i, p_r, u, v
+    double* sB = adj_cell_smem + 5 * RHS_NPT;  // [5][RHS_NPT] their cotangents
+    __shared__ double red[2][RHS_THREADS / 32];
+    if ((int)blockIdx.x >= nt) return;
+    const Tile t = tiles[blockIdx.x];
+    const Inst& I = insts[t.inst];
     if (has_error(I)) return;
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)I.nx * I.ny) return;
-    const int i = (int)(t / I.ny), j = (int)(t % I.ny);
-    const long long n = node_of(I, i, j);
-    if (!I.mask[n]) return;
     const DevParams& P = I.P;
     const long long plane = I.plane;
     const double* X = Xb + I.aoff;
     const double* rb = rbarb + I.aoff;
     double* W = Wb + I.aoff;
-    const double ob[3] = {rb[3 * plane + n], rb[4 * plane + n], rb[5 * plane + n]};
-    for (int dir = 0; dir < 2; ++dir) {
-        double pe[9], pi[9], pr[9], vel[9], s9[9][6];
-        for (int q = 0; q < 9; ++q) {
-            const long long m = dir == 0 ? node_of(I, i - 4 + q, j) : node_of(I, i, j - 4 + q);
-            load6(X, plane, m, s9[q]);
-            const Prim d = prim_from_state(s9[q], P);
-            pe[q] = d.pe; pi[q] = d.pi; pr[q] = d.pr; vel[q] = dir == 0 ? d.u : d.v;
+    const int nx = I.nx, ny = I.ny;
+    const int TJ = 1 << t.lg, TI = RHS_THREADS >> t.lg;
+    const int HJ = TJ + 8, NPT = (TI + 8) * HJ;
+    for (int p = threadIdx.x; p < NPT; p += blockDim.x) {
+        const int hi = p / HJ, hj = p - hi * HJ;
+        const bool corner = (hi < 4 || hi >= TI + 4) && (hj < 4 || hj >= TJ + 4);
+        const int i = t.i - 4 + hi, j = t.j0 - 4 + hj;
+        for (int q = 0; q < 5; ++q) sB[q * RHS_NPT + p] = 0.0;
+        if (corner || i < -RH3T_PAD || i >= nx + RH3T_PAD || j < -RH3T_PAD || j >= ny + RH3T_PAD) continue;
+        double s[6];
+        load6(X, plane, node_of(I, i, j), s);
+        const Prim d = prim_from_state(s, P);
+        sP[p] = d.pe; sP[RHS_NPT + p] = d.pi; sP[2 * RHS_NPT + p] = d.pr;
+        sP[3 * RHS_NPT + p] = d.u; sP[4 * RHS_NPT + p] = d.v;
+    }
+    __syncthreads();
+    const int ti = threadIdx.x >> t.lg, tj = threadIdx.x & (TJ - 1);
+    const int i = t.i + ti, j = t.j0 + tj;
+    double oei_b = 0.0, oer_b = 0.0;
+    if (i < nx && j < ny && I.mask[node_of(I, i, j)]) {
+        const long long n = node_of(I, i, j);
+        const double ob[3] = {rb[3 * plane + n], rb[4 * plane + n], rb[5 * plane + n]};
+        const int hc = (ti + 4) * HJ + (tj + 4);
+        for (int dir = 0; dir < 2; ++dir) {
+            const int step = dir == 0 ? HJ : 1;
+            double pe[9], pi[9], pr[9], vel[9];
+            for (int q = 0; q < 9; ++q) {
+                const int p = hc + (q - 4) * step;
+                pe[q] = sP[p]; pi[q] = sP[RHS_NPT + p]; pr[q] = sP[2 * RHS_NPT + p];
+                vel[q] = sP[(dir == 0 ? 3 : 4) * RHS_NPT + p];
+            }
+            double peb[9], pib[9], prb[9], velb[9];
+            noncon9_vjp(pe, pi, pr, vel, dir == 0 ? I.dx : I.dy, ob, peb, pib, prb, velb);
+            for (int q = 0; q < 9; ++q) {
+                const int p = hc + (q - 4) * step;
+                if (peb[q] != 0.0) atomicAdd(&sB[p], peb[q]);
+                if (pib[q] != 0.0) atomicAdd(&sB[RHS_NPT + p], pib[q]);
+                if (prb[q] != 0.0) atomicAdd(&sB[2 * RHS_NPT + p], prb[q]);
+                if (velb[q] != 0.0) atomicAdd(&sB[(dir == 0 ? 3 : 4) * RHS_NPT + p], velb[q]);
+            }
         }
-        double peb[9], pib[9], prb[9], velb[9];
-        noncon9_vjp(pe, pi, pr, vel, dir == 0 ? I.dx : I.dy, ob, peb, pib, prb, velb);
-        for (int q = 0; q < 9; ++q) {
+        if (I.source) { // source.rs:7-21
+            double s[6];
+            load6(X, plane, n, s);
+            double te, ti_, tr;
+            temps_from_state(s, P, te, ti_, tr);
+            const double oei = P.omega_ei, oer = P.omega_er;
+            const double te3 = te * te * te, tr3 = tr * tr * tr;
+            const double bte = -oei * ob[0] - oer * 4.0 * te3 * ob[0] + oei * ob[1] + oer * 4.0 * te3 * ob[2];
+            const double bti = oei * ob[0] - oei * ob[1];
+            const double btr = oer * 4.0 * tr3 * ob[0] - oer * 4.0 * tr3 * ob[2];
             double sb[6] = {0, 0, 0, 0, 0, 0};
-            prim_vjp(s9[q], P, dir == 0 ? velb[q] : 0.0, dir == 0 ? 0.0 : velb[q], 0.0, 0.0, 0.0, peb[q], pib[q],
-                     prb[q], sb);
-            const long long m = dir == 0 ? node_of(I, i - 4 + q, j) : node_of(I, i, j - 4 + q);
-            atomic_add6(W, plane, m, sb);
+            temps_vjp(s, P, bte, bti, btr, sb);
+            atomic_add6(W, plane, n, sb);
+            const double x4 = pow4d(te) - pow4d(tr);
+            oei_b = -(te - ti_) * ob[0] + (te - ti_) * ob[1];
+            oer_b = -x4 * ob[0] + x4 * ob[2];
         }
     }
-    if (I.source) { // source.rs:7-21
+    if (I.source) {
+        for (int o = 16; o > 0; o >>= 1) {
+            oei_b += __shfl_xor_sync(0xffffffffu, oei_b, o);
+            oer_b += __shfl_xor_sync(0xffffffffu, oer_b, o);
+        }
+        if ((threadIdx.x & 31) == 0) { red[0][threadIdx.x >> 5] = oei_b; red[1][threadIdx.x >> 5] = oer_b; }
+    }
+    __syncthreads();
+    if (I.source && threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        for (int w = 0; w < RHS_THREADS / 32; ++w) { a += red[0][w]; b += red[1][w]; }
+        if (a != 0.0) atomicAdd(&pbar[8 * t.inst + 6], a);
+        if (b != 0.0) atomicAdd(&pbar[8 * t.inst + 7], b);
+    }
+    // primitive cotangents -> state cotangents, one node each
+    for (int p = threadIdx.x; p < NPT; p += blockDim.x) {
+        const double b0 = sB[p], b1 = sB[RHS_NPT + p], b2 = sB[2 * RHS_NPT + p], b3 = sB[3 * RHS_NPT + p],
+                     b4 = sB[4 * RHS_NPT + p];
+        if (b0 == 0.0 && b1 == 0.0 && b2 == 0.0 && b3 == 0.0 && b4 == 0.0) continue;
+        const int hi = p / HJ, hj = p - hi * HJ;
+        const long long m = node_of(I, t.i - 4 + hi, t.j0 - 4 + hj);
         double s[6];
-        load6(X, plane, n, s);
-        double te, ti, tr;
-        temps_from_state(s, P, te, ti, tr);
-        const double oei = P.omega_ei, oer = P.omega_er;
-        const double te3 = te * te * te, tr3 = tr * tr * tr;
-        const double bte = -oei * ob[0] - oer * 4.0 * te3 * ob[0] + oei * ob[1] + oer * 4.0 * te3 * ob[2];
-        const double bti = oei * ob[0] - oei * ob[1];
-        const double btr = oer * 4.0 * tr3 * ob[0] - oer * 4.0 * tr3 * ob[2];
+        load6(X, plane, m, s);
         double sb[6] = {0, 0, 0, 0, 0, 0};
-        temps_vjp(s, P, bte, bti, btr, sb);
-        atomic_add6(W, plane, n, sb);
-        const double x4 = pow4d(te) - pow4d(tr);
-        atomicAdd(&pbar[8 * kk + 6], -(te - ti) * ob[0] + (te - ti) * ob[1]);
-        atomicAdd(&pbar[8 * kk + 7], -x4 * ob[0] + x4 * ob[2]);
+        prim_vjp(s, P, b3, b4, 0.0, 0.0, 0.0, b0, b1, b2, sb);
+        atomic_add6(W, plane, m, sb);
     }
 }
 
@@ -480,14 +797,28 @@ __constant__ int kAStOff[6] = {0, 1, 5, 14, 30, 55};
 __constant__ int kASOff[6] = {0, 1, 17, 98, 354, 979};
 __constant__ int kAWOff[6] = {0, 1, 9, 36, 100, 225};
 
+// the 90 dot products V^(k)_{c,r} = w_{r,k} . d_c as (c << 6) | (r << 3) | k,
+// longest first: lane l takes entries l, l + 32, l + 64
+__constant__ unsigned short kAdjVItems[90] = {
+    0x020, 0x021, 0x022, 0x023, 0x024, 0x060, 0x061, 0x062, 0x063, 0x064,
+    0x0a0, 0x0a1, 0x0a2, 0x0a3, 0x0a4, 0x0e0, 0x0e1, 0x0e2, 0x0e3, 0x0e4,
+    0x120, 0x121, 0x122, 0x123, 0x124, 0x160, 0x161, 0x162, 0x163, 0x164,
+    0x018, 0x019, 0x01a, 0x01b, 0x058, 0x059, 0x05a, 0x05b, 0x098, 0x099,
+    0x09a, 0x09b, 0x0d8, 0x0d9, 0x0da, 0x0db, 0x118, 0x119, 0x11a, 0x11b,
+    0x158, 0x159, 0x15a, 0x15b, 0x010, 0x011, 0x012, 0x050, 0x051, 0x052,
+    0x090, 0x091, 0x092, 0x0d0, 0x0d1, 0x0d2, 0x110, 0x111, 0x112, 0x150,
+    0x151, 0x152, 0x008, 0x009, 0x048, 0x049, 0x088, 0x089, 0x0c8, 0x0c9,
+    0x108, 0x109, 0x148, 0x149, 0x000, 0x040, 0x080, 0x0c0, 0x100, 0x140};
+
 struct AdjGhostWarp {
     double L[36], R[36], lam[6];             // L[6c + j]; R column c at R[6c + i]
+    double U6[6][56];                        // rotated stencil states
     double D[6][56], ACC[6][56], STD[6][56]; // STD becomes D-bar in place
-    double bb[6][5];
     double alpha[6][5], beta[6][5], V[6][5][5];
     double v[5][6], x[5][6], ub[5][6], xb[5][6], vinf[6], vinfb[6];
     double Lb[6][6], Rb[6][6];
     double vb[5][6];
+    double Z[6][6];
 };
 
 __device__ __forceinline__ int aorder(int a) { return a < 1 ? 0 : (a < 5 ? 1 : (a < 14 ? 2 : (a < 30 ? 3 : 4))); }
@@ -523,6 +854,7 @@ __device__ void ghost_vjp_warp(const Inst& I, const GhostRec& Rg, const double* 
         double s[6];
         load6(X, plane, st[a], s);
         const double u6[6] = {s[0], s[1] * nx + s[2] * ny, -s[1] * ny + s[2] * nx, s[3], s[4], s[5]};
+        for (int q = 0; q < 6; ++q) G.U6[q][a] = u6[q];
         for (int c = 0; c < 6; ++c) {
             double acc = 0.0;
             for (int q = 0; q < 6; ++q) acc += L[6 * c + q] * u6[q];
@@ -533,15 +865,18 @@ __device__ void ghost_vjp_warp(const Inst& I, const GhostRec& Rg, const double* 
     for (int a = lane; a < 55; a += 32) {
         const int r = aorder(a), m = (r + 1) * (r + 1), off = kAStOff[r], ar = a - off;
         const double* Sr = S + kASOff[r];
-        for (int c = 0; c < 6; ++c) {
-            double acc = 0.0, acct = 0.0;
-            for (int b = 0; b < m; ++b) {
-                acc += Sr[b * m + ar] * G.D[c][off + b];  // (S d)_a
-                acct += Sr[ar * m + b] * G.D[c][off + b]; // (S^T d)_a
+        double acc[6] = {0, 0, 0, 0, 0, 0}, acct[6] = {0, 0, 0, 0, 0, 0};
+        for (int b = 0; b < m; ++b) {
+            const double sab = Sr[b * m + ar], sba = Sr[ar * m + b]; // S[a][b], S[b][a]
+#pragma unroll
+            for (int c = 0; c < 6; ++c) {
+                const double d = G.D[c][off + b];
+                acc[c] += sab * d;  // (S d)_a
+                acct[c] += sba * d; // (S^T d)_a
             }
-            G.ACC[c][a] = acc;
-            G.STD[c][a] = acct;
         }
+#pragma unroll
+        for (int c = 0; c < 6; ++c) { G.ACC[c][a] = acc[c]; G.STD[c][a] = acct[c]; }
     }
     __syncwarp();
     if (lane < 30) {
@@ -550,15 +885,21 @@ __device__ void ghost_vjp_warp(const Inst& I, const GhostRec& Rg, const double* 
         double beta = 0.0;
         for (int a = 0; a < m; ++a) beta += G.D[c][off + a] * G.ACC[c][off + a];
         G.beta[c][r] = beta;
-        G.alpha[c][r] = rec[GH_D + r] / pow_q(P.eps + beta, P.weno_q);
-        for (int k = 0; k < 5; ++k) {
-            double v = 0.0;
-            if (k <= r) {
-                const double* w = rec + GH_W + kAWOff[r] + k * m;
-                for (int a = 0; a < m; ++a) v += w[a] * G.D[c][off + a];
-            }
-            G.V[c][r][k] = v;
-        }
+        const double x = P.eps + beta;
+        double xq;
+        if (P.weno_q == 10.0) { const double x2 = x * x, x4 = x2 * x2, x8 = x4 * x4; xq = x8 * x2; }
+        else xq = pow(x, P.weno_q);
+        G.alpha[c][r] = rec[GH_D + r] / xq;
+        for (int k = r + 1; k < 5; ++k) G.V[c][r][k] = 0.0;
+    }
+    for (int q = lane; q < 90; q += 32) {
+        const unsigned e = kAdjVItems[q];
+        const int c = (int)(e >> 6), r = (int)((e >> 3) & 7u), k = (int)(e & 7u);
+        const int m = (r + 1) * (r + 1), off = kAStOff[r];
+        const double* w = rec + GH_W + kAWOff[r] + k * m;
+        double v = 0.0;
+        for (int a = 0; a < m; ++a) v += w[a] * G.D[c][off + a];
+        G.V[c][r][k] = v;
     }
     __syncwarp();
     if (lane < 30) {
@@ -667,15 +1008,7 @@ __device__ void ghost_vjp_warp(const Inst& I, const GhostRec& Rg, const double* 
     for (int e = lane; e < 36; e += 32) {
         const int c = e / 6, q = e - 6 * (e / 6);
         double acc = 0.0;
-        for (int a = 0; a < 55; ++a) {
-            const long long na = st[a];
-            const double s1 = X[plane + na], s2 = X[2 * plane + na];
-            const double uq = q == 0 ? X[na]
-                              : q == 1 ? s1 * nx + s2 * ny
-                              : q == 2 ? -s1 * ny + s2 * nx
-                                       : X[q * plane + na];
-            acc += G.STD[c][a] * uq;
-        }
+        for (int a = 0; a < 55; ++a) acc += G.STD[c][a] * G.U6[q][a];
         G.Lb[c][q] += acc;
     }
     for (int a = lane; a < 55; a += 32) {
@@ -689,37 +1022,38 @@ __device__ void ghost_vjp_warp(const Inst& I, const GhostRec& Rg, const double* 
         atomic_add6(Ub, plane, st[a], sb);
     }
     __syncwarp();
-    // L, R of the nearest node: Roe base of two equal rotated states
-    if (lane < 6) {
-        double s[6];
-        load6(X, plane, Rg.src, s);
-        const double q6[6] = {s[0], s[1] * nx + s[2] * ny, -s[1] * ny + s[2] * nx, s[3], s[4], s[5]};
-        const Prim d1 = prim_from_state(q6, P);
-        const Roe q = roe_average(q6[0], d1, q6[0], d1, P);
-        const double base[5] = {q.u, q.v, q.ee, q.ei, q.er};
-        double bb[5] = {0, 0, 0, 0, 0};
-        lr_base_vjp<0>(lane, base, P, G.Lb[lane], G.Rb[lane], 0.0, bb);
-        for (int m = 0; m < 5; ++m) G.bb[lane][m] = bb[m];
+    // L, R of the nearest node: L-bar folded into R-bar (lanes over the 36
+    // entries), then the Roe base of two equal rotated states
+    for (int e = lane; e < 36; e += 32) {
+        const int j = e / 6, c = e - 6 * (e / 6);
+        double acc = 0.0;
+        for (int k = 0; k < 6; ++k) acc += G.Lb[j][k] * L[6 * c + k];
+        G.Z[j][c] = acc;
+    }
+    __syncwarp();
+    for (int e = lane; e < 36; e += 32) {
+        const int c = e / 6, i = e - 6 * (e / 6);
+        double acc = 0.0;
+        for (int j = 0; j < 6; ++j) acc += L[6 * j + i] * G.Z[j][c];
+        G.Rb[c][i] -= acc;
     }
     __syncwarp();
     if (lane == 0) {
         double s[6];
         load6(X, plane, Rg.src, s);
         const double q6[6] = {s[0], s[1] * nx + s[2] * ny, -s[1] * ny + s[2] * nx, s[3], s[4], s[5]};
-        double bb[5];
-        for (int m = 0; m < 5; ++m) {
-            double acc = 0.0;
-            for (int c = 0; c < 6; ++c) acc += G.bb[c][m];
-            bb[m] = acc;
-        }
-        {
-            double ga[6] = {0, 0, 0, 0, 0, 0}, gb2[6] = {0, 0, 0, 0, 0, 0};
-            roe_vjp(q6, q6, P, bb, ga, gb2);
-            double gr[6];
-            for (int c = 0; c < 6; ++c) gr[c] = ga[c] + gb2[c];
-            const double sb[6] = {gr[0], gr[1] * nx - gr[2] * ny, gr[1] * ny + gr[2] * nx, gr[3], gr[4], gr[5]};
-            atomic_add6(Ub, plane, Rg.src, sb);
-        }
+        const Prim d1 = prim_from_state(q6, P);
+        const Roe q = roe_average(q6[0], d1, q6[0], d1, P);
+        const double base[5] = {q.u, q.v, q.ee, q.ei, q.er};
+        const double lamb[6] = {0, 0, 0, 0, 0, 0};
+        double bb[5] = {0, 0, 0, 0, 0};
+        r_base_vjp<0>(base, P, G.Rb, lamb, bb);
+        double ga[6] = {0, 0, 0, 0, 0, 0}, gb2[6] = {0, 0, 0, 0, 0, 0};
+        roe_vjp(q6, q6, P, bb, ga, gb2);
+        double gr[6];
+        for (int c = 0; c < 6; ++c) gr[c] = ga[c] + gb2[c];
+        const double sb[6] = {gr[0], gr[1] * nx - gr[2] * ny, gr[1] * ny + gr[2] * nx, gr[3], gr[4], gr[5]};
+        atomic_add6(Ub, plane, Rg.src, sb);
     }
 }
 
@@ -779,21 +1113,28 @@ __global__ void k_adj_fluid(const Inst* __restrict__ insts, int k0, const double
 }
 
 // ---------------------------------------------------------------- launchers
-void launch_adj_l(cudaStream_t s, const Inst* insts, int k0, int n, long long max_cells, long long max_faces,
-                  const GhostRec* heavy, int nh, const GhostRec* cheap, int nc, const double* hrec, const double* X,
-                  const double* rbar, double* W, double* Ub, double* pbar) {
+void launch_adj_l(cudaStream_t s, const Inst* insts, int k0, int n, long long max_cells, const Tile* tx, int ntx,
+                  const Tile* ty, int nty, const Tile* tr, int ntr, const GhostRec* heavy, int nh,
+                  const GhostRec* cheap, int nc, const double* hrec, const double* X, const double* rbar, double* W,
+                  double* Ub, double* pbar) {
     if (n <= 0) return;
-    const unsigned fb = (unsigned)((max_faces + 127) / 128), cb = (unsigned)((max_cells + 127) / 128);
-    k_adj_faces<<<dim3(fb, n), 128, 0, s>>>(insts, k0, X, rbar, W, 0);
-    k_adj_faces<<<dim3(fb, n), 128, 0, s>>>(insts, k0, X, rbar, W, 1);
-    k_adj_cells<<<dim3(cb, n), 128, 0, s>>>(insts, k0, X, rbar, W, pbar);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_adj_cells, cudaFuncAttributeMaxDynamicSharedMemorySize, ADJ_CELL_SMEM);
+        cudaFuncSetAttribute(k_adj_flux, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(AdjFluxShared));
+        attr = true;
+    }
+    const unsigned cb = (unsigned)((max_cells + 127) / 128);
+    if (ntx + nty > 0)
+        k_adj_flux<<<ntx + nty, FLUX_THREADS, sizeof(AdjFluxShared), s>>>(insts, tx, ntx, ty, nty, X, rbar, W);
+    if (ntr > 0) k_adj_cells<<<ntr, RHS_THREADS, ADJ_CELL_SMEM, s>>>(insts, tr, ntr, X, rbar, W, pbar);
     const int nbh = (nh + AG_WARPS - 1) / AG_WARPS, nbc = (nc + AG_WARPS * 32 - 1) / (AG_WARPS * 32);
     if (nbh + nbc > 0)
         k_adj_ghosts<<<nbh + nbc, AG_WARPS * 32, 0, s>>>(insts, heavy, nh, cheap, nc, hrec, X, W, Ub, pbar, nbh);
     k_adj_fluid<<<dim3(cb, n), 128, 0, s>>>(insts, k0, W, Ub);
 }
 
-int adj_l_launches(int nh, int nc) { return 4 + (nh + nc > 0 ? 1 : 0); }
+int adj_l_launches(int nh, int nc) { return 3 + (nh + nc > 0 ? 1 : 0); }
 
 // ---------------------------------------------------------------- RK3 step plumbing
 // copy the 6 planes of stage buffer `which` (0 U, 1 A, 2 B) of instances
@@ -871,35 +1212,45 @@ __global__ void __launch_bounds__(256) k_adj_stage(const Inst* __restrict__ inst
 
 // dt = cfl * min_cells local_dt(u0) (main.rs:375-408, dt.rs:5-34): the
 // derivative goes to the first cell, in i*ny+j order, whose local dt equals
-// the minimum; one block per instance. Steps whose dt was clipped to t_final
-// have none.
-__global__ void __launch_bounds__(256) k_adj_dt(const Inst* __restrict__ insts, int k0, const double* __restrict__ X,
-                                                const DevScalars* __restrict__ sc, const double* __restrict__ dtbar,
-                                                double* __restrict__ U0, double* __restrict__ pbar) {
-    __shared__ long long best;
-    const int k = k0 + blockIdx.x;
+// the minimum. Steps whose dt was clipped to t_final have none.
+// k_adj_dt_find: that cell's index per instance (argmin initialised to ~0).
+__global__ void __launch_bounds__(256) k_adj_dt_find(const Inst* __restrict__ insts, int k0,
+                                                     const double* __restrict__ X, const DevScalars* __restrict__ sc,
+                                                     const double* __restrict__ dtbar,
+                                                     unsigned long long* __restrict__ argmin) {
+    const int k = k0 + blockIdx.y;
     const Inst& I = insts[k];
     const DevScalars& S = sc[k];
-    const double cfl = S.cfl_factor;
-    if (!(S.dt == cfl * S.dt_cfl) || dtbar[k] == 0.0) return;
-    if (threadIdx.x == 0) best = (long long)I.nx * I.ny;
-    __syncthreads();
+    if (!(S.dt == S.cfl_factor * S.dt_cfl) || dtbar[k] == 0.0) return;
+    const long long l = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= (long long)I.nx * I.ny) return;
+    const long long n = node_of(I, (int)(l / I.ny), (int)(l % I.ny));
+    if (!I.mask[n]) return;
+    double s[6];
+    load6(X + I.aoff, I.plane, n, s);
+    if (local_dt(s, I.dx, I.dy, I.P) == S.dt_cfl) atomicMin(&argmin[k], (unsigned long long)l);
+}
+
+// k_adj_dt_apply: one thread per instance, dual numbers in the state and omegas
+__global__ void k_adj_dt_apply(const Inst* __restrict__ insts, int k0, int n, const double* __restrict__ X,
+                               const DevScalars* __restrict__ sc, const double* __restrict__ dtbar,
+                               const unsigned long long* __restrict__ argmin, double* __restrict__ U0,
+                               double* __restrict__ pbar) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    const int k = k0 + q;
+    const Inst& I = insts[k];
+    const DevScalars& S = sc[k];
+    if (!(S.dt == S.cfl_factor * S.dt_cfl) || dtbar[k] == 0.0) return;
+    const unsigned long long l = argmin[k];
+    if (l >= (unsigned long long)I.nx * I.ny) return;
+    const long long nd = node_of(I, (int)(l / I.ny), (int)(l % I.ny));
     const double* x = X + I.aoff;
-    for (long long l = threadIdx.x; l < (long long)I.nx * I.ny; l += blockDim.x) {
-        const long long n = node_of(I, (int)(l / I.ny), (int)(l % I.ny));
-        if (!I.mask[n]) continue;
-        double s[6];
-        load6(x, I.plane, n, s);
-        if (local_dt(s, I.dx, I.dy, I.P) == S.dt_cfl) atomicMin(&best, l);
-    }
-    __syncthreads();
-    if (threadIdx.x != 0 || best >= (long long)I.nx * I.ny) return;
-    const long long n = node_of(I, (int)(best / I.ny), (int)(best % I.ny));
     D8 s8[6];
-    for (int c = 0; c < 6; ++c) s8[c] = D8::var(x[c * I.plane + n], c);
+    for (int c = 0; c < 6; ++c) s8[c] = D8::var(x[c * I.plane + nd], c);
     const D8 d = local_dt_t<D8>(s8, I.dx, I.dy, I.P, D8::var(I.P.omega_ei, 6), D8::var(I.P.omega_er, 7));
-    const double g = cfl * dtbar[k];
-    for (int c = 0; c < 6; ++c) U0[I.aoff + c * I.plane + n] += g * d.d[c];
+    const double g = S.cfl_factor * dtbar[k];
+    for (int c = 0; c < 6; ++c) U0[I.aoff + c * I.plane + nd] += g * d.d[c];
     pbar[8 * k + 6] += g * d.d[6];
     pbar[8 * k + 7] += g * d.d[7];
 }
@@ -921,10 +1272,12 @@ void launch_adj_stage(cudaStream_t s, const Inst* insts, int k0, int n, long lon
     k_adj_stage<<<dim3((unsigned)((max_cells + 255) / 256), n), 256, 0, s>>>(insts, k0, stage, Y, U0, Uin, rbar, R,
                                                                              sc, dtbar);
 }
-void launch_adj_dt(cudaStream_t s, const Inst* insts, int k0, int n, const double* X, const DevScalars* sc,
-                   const double* dtbar, double* U0, double* pbar) {
+void launch_adj_dt(cudaStream_t s, const Inst* insts, int k0, int n, long long max_cells, const double* X,
+                   const DevScalars* sc, const double* dtbar, unsigned long long* argmin, double* U0, double* pbar) {
     if (n <= 0) return;
-    k_adj_dt<<<n, 256, 0, s>>>(insts, k0, X, sc, dtbar, U0, pbar);
+    cudaMemsetAsync(argmin + k0, 0xff, (size_t)n * sizeof(unsigned long long), s);
+    k_adj_dt_find<<<dim3((unsigned)((max_cells + 255) / 256), n), 256, 0, s>>>(insts, k0, X, sc, dtbar, argmin);
+    k_adj_dt_apply<<<(n + 63) / 64, 64, 0, s>>>(insts, k0, n, X, sc, dtbar, argmin, U0, pbar);
 }
 
 } // namespace rh3t

@@ -35,13 +35,15 @@ struct AdjBuffers {
     double *Y = nullptr, *U0 = nullptr, *U1 = nullptr, *U2 = nullptr, *W = nullptr, *rbar = nullptr;
     double* pbar = nullptr;     // n_inst x 8
     double* dtbar = nullptr;    // n_inst
+    unsigned long long* argmin = nullptr; // n_inst: the dt-minimising cell
 };
 
 namespace rh3t {
 void adj_free(rh3t_ctx* c) {
     AdjBuffers* a = c->adj;
     if (!a) return;
-    void* ptrs[] = {a->ckpt, a->ckpt_sc, a->seg, a->seg_sc, a->Y, a->U0, a->U1, a->U2, a->W, a->rbar, a->pbar, a->dtbar};
+    void* ptrs[] = {a->ckpt, a->ckpt_sc, a->seg,  a->seg_sc, a->Y,     a->U0,
+                    a->U1,   a->U2,      a->W,    a->rbar,   a->pbar, a->dtbar, a->argmin};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete a;
@@ -81,6 +83,7 @@ int ensure_work(rh3t_ctx* c) {
     }
     CK(c, cudaMalloc(&a->pbar, (size_t)c->n_inst * 8 * sizeof(double)));
     CK(c, cudaMalloc(&a->dtbar, (size_t)c->n_inst * sizeof(double)));
+    CK(c, cudaMalloc(&a->argmin, (size_t)c->n_inst * sizeof(unsigned long long)));
     return RH3T_OK;
 }
 
@@ -96,8 +99,8 @@ void enqueue_vjp_l(rh3t_ctx* c, const double* X, const double* rbar, double* Ub)
     cudaMemsetAsync(a->W, 0, (size_t)c->total_planes * sizeof(double), c->stream);
     int nh, nc;
     ghost_ranges(c, nh, nc);
-    launch_adj_l(c->stream, c->d_inst, 0, c->n_inst, c->max_cells, c->max_faces, c->d_gpart, nh,
-                 c->d_gpart + c->n_gheavy, nc, c->d_hrec, X, rbar, a->W, Ub, a->pbar);
+    launch_adj_l(c->stream, c->d_inst, 0, c->n_inst, c->max_cells, c->d_tx, c->ntx, c->d_ty, c->nty, c->d_tr, c->ntr,
+                 c->d_gpart, nh, c->d_gpart + c->n_gheavy, nc, c->d_hrec, X, rbar, a->W, Ub, a->pbar);
     c->launches += adj_l_launches(nh, nc);
 }
 
@@ -246,8 +249,8 @@ extern "C" int rh3t_adjoint_backward(rh3t_ctx* c, const double* dJ_du, double* d
             launch_adj_stage(s, c->d_inst, 0, c->n_inst, c->max_cells, 0, a->U1, a->U0, nullptr, a->rbar,
                              rec + 3 * np, sc, a->dtbar);
             enqueue_vjp_l(c, rec, a->rbar, a->U0);
-            launch_adj_dt(s, c->d_inst, 0, c->n_inst, rec, sc, a->dtbar, a->U0, a->pbar);
-            c->launches += 4;
+            launch_adj_dt(s, c->d_inst, 0, c->n_inst, c->max_cells, rec, sc, a->dtbar, a->argmin, a->U0, a->pbar);
+            c->launches += 5;
             std::swap(a->Y, a->U0);
         }
         CK(c, cudaGetLastError());

@@ -58,10 +58,10 @@ template <int N> __device__ __forceinline__ DualN<N> operator*(const DualN<N>& a
     return r;
 }
 template <int N> __device__ __forceinline__ DualN<N> operator/(const DualN<N>& a, const DualN<N>& b) {
-    const double q = a.v / b.v;
+    const double q = a.v / b.v, ib = 1.0 / b.v;
     DualN<N> r(q);
 #pragma unroll
-    for (int k = 0; k < N; ++k) r.d[k] = (a.d[k] - q * b.d[k]) / b.v;
+    for (int k = 0; k < N; ++k) r.d[k] = (a.d[k] - q * b.d[k]) * ib;
     return r;
 }
 template <int N> __device__ __forceinline__ DualN<N> operator+(const DualN<N>& a, double b) { return a + DualN<N>(b); }
@@ -80,14 +80,26 @@ template <int N> __device__ __forceinline__ DualN<N> operator*(double a, const D
     for (int k = 0; k < N; ++k) r.d[k] = a * b.d[k];
     return r;
 }
-template <int N> __device__ __forceinline__ DualN<N> operator/(const DualN<N>& a, double b) { return a / DualN<N>(b); }
-template <int N> __device__ __forceinline__ DualN<N> operator/(double a, const DualN<N>& b) { return DualN<N>(a) / b; }
+template <int N> __device__ __forceinline__ DualN<N> operator/(const DualN<N>& a, double b) {
+    const double ib = 1.0 / b;
+    DualN<N> r(a.v / b);
+#pragma unroll
+    for (int k = 0; k < N; ++k) r.d[k] = a.d[k] * ib;
+    return r;
+}
+template <int N> __device__ __forceinline__ DualN<N> operator/(double a, const DualN<N>& b) {
+    const double q = a / b.v, f = -q / b.v;
+    DualN<N> r(q);
+#pragma unroll
+    for (int k = 0; k < N; ++k) r.d[k] = f * b.d[k];
+    return r;
+}
 
 template <int N> __device__ __forceinline__ DualN<N> sqrt(const DualN<N>& a) {
-    const double s = ::sqrt(a.v);
+    const double s = ::sqrt(a.v), h = 0.5 / s;
     DualN<N> r(s);
 #pragma unroll
-    for (int k = 0; k < N; ++k) r.d[k] = a.d[k] / (2.0 * s);
+    for (int k = 0; k < N; ++k) r.d[k] = a.d[k] * h;
     return r;
 }
 template <int N> __device__ __forceinline__ DualN<N> fabs(const DualN<N>& a) { return a.v < 0.0 ? -a : a; }

@@ -23,9 +23,11 @@ void launch_ghost_values(cudaStream_t s, const Inst* insts, const GhostRec* recs
 void launch_dfma(cudaStream_t s, int blocks, double* out, int iters);
 // adjoint (adjoint.cu): plane sets are batch-wide arrays of 6 padded planes
 // per instance at Inst::aoff
-void launch_adj_l(cudaStream_t s, const Inst* insts, int k0, int n, long long max_cells, long long max_faces,
-                  const GhostRec* heavy, int nh, const GhostRec* cheap, int nc, const double* hrec, const double* X,
-                  const double* rbar, double* W, double* Ub, double* pbar);
+// tx, ty, tr: the face and RHS tiles of instances [k0, k0 + n)
+void launch_adj_l(cudaStream_t s, const Inst* insts, int k0, int n, long long max_cells, const Tile* tx, int ntx,
+                  const Tile* ty, int nty, const Tile* tr, int ntr, const GhostRec* heavy, int nh,
+                  const GhostRec* cheap, int nc, const double* hrec, const double* X, const double* rbar, double* W,
+                  double* Ub, double* pbar);
 int adj_l_launches(int nh, int nc);
 void launch_adj_copy(cudaStream_t s, const Inst* insts, int k0, int n, long long max_plane, int which, double* set,
                      int dir);
@@ -34,7 +36,7 @@ void launch_adj_aos(cudaStream_t s, const Inst* insts, int k0, int n, long long 
 void launch_adj_stage(cudaStream_t s, const Inst* insts, int k0, int n, long long max_cells, int stage,
                       const double* Y, double* U0, double* Uin, double* rbar, const double* R, const DevScalars* sc,
                       double* dtbar);
-void launch_adj_dt(cudaStream_t s, const Inst* insts, int k0, int n, const double* X, const DevScalars* sc,
-                   const double* dtbar, double* U0, double* pbar);
+void launch_adj_dt(cudaStream_t s, const Inst* insts, int k0, int n, long long max_cells, const double* X,
+                   const DevScalars* sc, const double* dtbar, unsigned long long* argmin, double* U0, double* pbar);
 void launch_math_check(cudaStream_t s, const double* x, int n, double q, double* out);
 } // namespace rh3t

@@ -224,6 +224,62 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def adjoint_bench(rh, torch, local, exact, nsteps=200, ckpt=20, n=32):
+    """The adjoint workload: n seeded 121x481 half-cylinders (Mach U[2,4],
+    exchange coefficients log-U[0.1,10]), J = surface pressure on the arc
+    after nsteps, gradient with respect to the Mach number, the two exchange
+    coefficients and the initial state, checkpoints every ckpt steps; device
+    times of the forward solve and of the adjoint (checkpointed forward +
+    reverse sweep)."""
+    specs = rh.cases.batch_specs(n, sizes=(121,))
+    fields = [rh.cases.batch_field(sp) for sp in specs]
+    grids = [rh.GhostGrid.build(f) for f in fields]
+    Js = [rh.cases.SurfacePressure(f, g) for f, g in zip(fields, grids)]
+    dev = torch.device(f"cuda:{local}")
+
+    def timed(fn, b):
+        st = torch.cuda.ExternalStream(b.stream, device=dev)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record(st)
+        out = fn()
+        e1.record(st)
+        torch.cuda.synchronize()
+        return out, e0.elapsed_time(e1), 1e3 * (time.perf_counter() - t0)
+
+    fwd = rh.Batch(fields, grids, device=local, exact=exact)
+    fwd.advance(3, CFL)  # warm-up (graph capture)
+    fwd.upload(fields)
+    _, f_ms, f_wall = timed(lambda: fwd.advance(nsteps, CFL), fwd)
+    fwd.close()
+    b = rh.Batch(fields, grids, device=local, exact=exact)
+    b.adjoint_forward(2, CFL, 2)  # warm-up: buffers, graph
+    b.adjoint_backward([np.zeros((int(c), 6)) for c in b.cells])
+    b.upload(fields)
+
+    def adjoint():
+        b.adjoint_forward(nsteps, CFL, ckpt)
+        res = b.download()
+        lam = [J.grad(u) for J, (u, _) in zip(Js, res)]
+        return res, b.adjoint_backward(lam)
+
+    (res, (g0, gp)), a_ms, a_wall = timed(adjoint, b)
+    dmach = []
+    for k, sp in enumerate(specs):
+        hm = 1e-7
+        dudm = (rh.cases.freestream(sp["mach"] + hm) - rh.cases.freestream(sp["mach"] - hm)) / (2 * hm)
+        dmach.append(float(gp[k, :6] @ dudm) + float((g0[k][fields[k].fluid] @ dudm).sum()))
+    b.close()
+    return {"workload": f"{n} half-cylinder instances 121x481, Mach U[2,4], omega log-U[0.1,10] x 1.0, "
+                        f"seed 20261203; J = surface pressure on the arc after {nsteps} steps; gradient in Mach, "
+                        f"omega_ei, omega_er and the initial state; checkpoints every {ckpt} steps",
+            "forward_ms": f_ms, "adjoint_ms": a_ms, "adj_fwd_ratio": a_ms / f_ms,
+            "wall_ms": {"forward": f_wall, "adjoint": a_wall},
+            "J_first": float(Js[0].value(res[0][0])), "dJ_dMach_first": dmach[0],
+            "dJ_domega_first": [float(gp[0, 6]), float(gp[0, 7])]}
+
+
 def run_batch(args, rh, flops, torch, dist, world, rank, local):
     """Batched workload: all instances in one Batch, one CUDA graph per step;
     then the plain solver on the same instances one at a time."""
@@ -304,6 +360,10 @@ def run_batch(args, rh, flops, torch, dist, world, rank, local):
                "call": "rh3t_upload_batch + rh3t_advance(1 step) + rh3t_download_batch (all Field::value arrays)",
                "steps": k_e2e}
 
+    adj = None
+    if not args.no_adjoint:
+        adj = adjoint_bench(rh, torch, local, args.exact)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         from oracle import oracle as O  # timed CPU baseline only
@@ -330,6 +390,7 @@ def run_batch(args, rh, flops, torch, dist, world, rank, local):
             "instances_per_s": value / cells * b.n,
             "plain_one_at_a_time": {"value": plain_value, "unit": "cell-updates/s", "steps_per_instance": k_plain,
                                     "batched_speedup": value / plain_value},
+            "adjoint": adj,
             "roofline": {"bound": "fp64", "kernel": "k_flux (x+y interface WENO5 fluxes, all instances)",
                          "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                          "traffic": FLUX_TRAFFIC_BYTES.get(args.workload) if not args.exact else None,
@@ -357,6 +418,7 @@ def main():
     ap.add_argument("--exact", action="store_true", help="bench the no-FMA-contraction build")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

@@ -5,8 +5,9 @@ rh3t_adjoint_forward / rh3t_adjoint_backward).
     l() (oracle/src/jvp.hpp) on the 31 x 121 half-cylinder: for random
     cotangents rbar and directions du (state), du_inf (FarField state) and
     domega (exchange coefficients), <rbar, J du> = <J^T rbar, du> to a
-    relative 1e-10 (no-contraction build: both sides take the same branches
-    at the kinks);
+    relative 1e-9 (no-contraction build: both sides take the same branches at
+    the kinks; the derivatives of the WENO weights, ~(eps + beta)^-3, amplify
+    the adjoint's own roundings to ~1e-10 of the sum);
   - time loop, against FP64 central finite differences (h = 1e-6 relative)
     of J = surface pressure on the arc (cases.SurfacePressure) after N steps,
     with respect to the inflow Mach number and the two exchange coefficients
@@ -55,7 +56,7 @@ def test_l_vjp_matches_dual_oracle(rh, O, which):
     if dom is not None:
         rhs += float(pb[6:] @ dom)
     print(f"{which}: <rbar, J du> = {lhs:.15e}, <J^T rbar, du> = {rhs:.15e}")
-    assert abs(lhs - rhs) <= 1e-10 * max(abs(lhs), 1e-300)
+    assert abs(lhs - rhs) <= 1e-9 * max(abs(lhs), 1e-300)
 
 
 def test_l_vjp_fma_build_close(rh, O):
@@ -177,5 +178,6 @@ def test_batch_adjoint_equals_single(rh):
         u, _ = s.download(0)
         assert np.array_equal(u, res[k][0])
         a0, ap = s.adjoint_backward([J.grad(u)])
-        assert np.abs(a0[0] - g0[k]).max() <= 1e-12 * np.abs(a0[0]).max()
-        assert np.abs(ap[0] - gp[k]).max() <= 1e-12 * np.abs(ap[0]).max()
+        # atomic accumulation: the order of the additions differs between runs
+        assert np.abs(a0[0] - g0[k]).max() <= 1e-10 * np.abs(a0[0]).max()
+        assert np.abs(ap[0] - gp[k]).max() <= 1e-10 * np.abs(ap[0]).max()
