@@ -15,7 +15,8 @@ STATUS_NAMES = {
 
 # exported symbols of include/rh3t.h
 EXPORTS = (
-    "rh3t_geom_create", "rh3t_geom_fluid_mask", "rh3t_geom_build_ghosts", "rh3t_geom_ghost_table",
+    "rh3t_geom_create", "rh3t_geom_fluid_mask", "rh3t_geom_build_ghosts", "rh3t_geom_build_ghosts_device",
+    "rh3t_geom_ghost_table",
     "rh3t_geom_access_table", "rh3t_geom_last_error", "rh3t_geom_destroy", "rh3t_default_params", "rh3t_create",
     "rh3t_upload_state", "rh3t_download_state", "rh3t_l", "rh3t_calc_global_dt", "rh3t_rk3_ssp", "rh3t_advance",
     "rh3t_step_host", "rh3t_last_dt", "rh3t_profile_steps", "rh3t_fp64_peak", "rh3t_math_check",
@@ -97,6 +98,7 @@ def load(exact=False):
                                  C.c_int32, V, P(V)]),
         "rh3t_geom_fluid_mask": (I, [V, V]),
         "rh3t_geom_build_ghosts": (I, [V, C.c_int32]),
+        "rh3t_geom_build_ghosts_device": (I, [C.c_int32, V, C.c_int32, C.c_int32]),
         "rh3t_geom_ghost_table": (I, [V, P(GhostTable)]),
         "rh3t_geom_access_table": (I, [V, V]),
         "rh3t_geom_last_error": (C.c_char_p, [V]),

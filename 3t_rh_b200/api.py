@@ -286,36 +286,63 @@ class GhostGrid:
     Wall / Outflow / FarField ghosts the GhostBC tables (bc1.rs:50-57)."""
 
     @classmethod
-    def build(cls, field, n_threads=0, with_access=False):
-        g = cls()
+    def build(cls, field, n_threads=0, with_access=False, device=None):
+        """GhostGrid::build (ghost.rs:50-118). device=None builds every table
+        on the host; a device index computes the least-squares tables
+        (bc1.rs:108-188) on that GPU (bit-identical results)."""
+        if device is not None:
+            return cls.build_many([field], device=device, n_threads=n_threads, with_access=with_access)[0]
         with _Geom(field) as geom:
             rc = geom.L.rh3t_geom_build_ghosts(geom.h, n_threads)
             if rc:
                 raise RH3TError(rc, geom.L.rh3t_geom_last_error(geom.h).decode())
-            v = _lib.GhostTable()
-            geom.L.rh3t_geom_ghost_table(geom.h, C.byref(v))
-            n, m = v.n_ghosts, v.n_heavy
+            return cls._from_geom(geom, field, with_access)
 
-            def cp(ptr, count, dtype):
-                if count == 0:
-                    return np.zeros(0, dtype=dtype)
-                buf = (C.c_char * (count * np.dtype(dtype).itemsize)).from_address(ptr)
-                return np.frombuffer(buf, dtype=dtype).copy()
+    @classmethod
+    def build_many(cls, fields, device=0, n_threads=0, with_access=False):
+        """GhostGrid::build of many fields at once, the least-squares tables of
+        all their Wall / Outflow / FarField ghosts computed in one pass on
+        GPU `device` (rh3t_geom_build_ghosts_device)."""
+        geoms = [_Geom(f) for f in fields]
+        try:
+            L = geoms[0].L
+            arr = (C.c_void_p * len(geoms))(*[g.h.value for g in geoms])
+            rc = L.rh3t_geom_build_ghosts_device(len(geoms), arr, n_threads, device)
+            if rc:
+                msg = next((L.rh3t_geom_last_error(g.h).decode() for g in geoms if L.rh3t_geom_last_error(g.h)), "")
+                raise RH3TError(rc, msg or "device ghost-grid build failed")
+            return [cls._from_geom(g, f, with_access) for g, f in zip(geoms, fields)]
+        finally:
+            for g in geoms:
+                g.close()
 
-            g.idx = cp(v.idx, 2 * n, np.int32).reshape(n, 2)
-            g.boundary = cp(v.boundary, n, np.int32)
-            g.side = cp(v.side, n, np.int32)
-            g.proj = cp(v.proj, 5 * n, np.float64).reshape(n, 5)
-            g.pre = cp(v.pre, n, np.int32)
-            g.nearest = cp(v.nearest, 2 * m, np.int32).reshape(m, 2)
-            g.stencil = cp(v.stencil, 55 * m, np.uint32).reshape(m, 55)
-            g.s = cp(v.s, 979 * m, np.float64).reshape(m, 979)
-            g.w = cp(v.w, 225 * m, np.float64).reshape(m, 225)
-            g.d = cp(v.d, 5 * m, np.float64).reshape(m, 5)
-            if with_access:
-                g.access = np.zeros(field.grid.len() * 17, np.uint32)
-                geom.L.rh3t_geom_access_table(geom.h, g.access.ctypes.data)
-                g.access = g.access.reshape(-1, 17)
+    @classmethod
+    def _from_geom(cls, geom, field, with_access):
+        g = cls()
+        v = _lib.GhostTable()
+        geom.L.rh3t_geom_ghost_table(geom.h, C.byref(v))
+        n, m = v.n_ghosts, v.n_heavy
+
+        def cp(ptr, count, dtype):
+            if count == 0:
+                return np.zeros(0, dtype=dtype)
+            buf = (C.c_char * (count * np.dtype(dtype).itemsize)).from_address(ptr)
+            return np.frombuffer(buf, dtype=dtype).copy()
+
+        g.idx = cp(v.idx, 2 * n, np.int32).reshape(n, 2)
+        g.boundary = cp(v.boundary, n, np.int32)
+        g.side = cp(v.side, n, np.int32)
+        g.proj = cp(v.proj, 5 * n, np.float64).reshape(n, 5)
+        g.pre = cp(v.pre, n, np.int32)
+        g.nearest = cp(v.nearest, 2 * m, np.int32).reshape(m, 2)
+        g.stencil = cp(v.stencil, 55 * m, np.uint32).reshape(m, 55)
+        g.s = cp(v.s, 979 * m, np.float64).reshape(m, 979)
+        g.w = cp(v.w, 225 * m, np.float64).reshape(m, 225)
+        g.d = cp(v.d, 5 * m, np.float64).reshape(m, 5)
+        if with_access:
+            g.access = np.zeros(field.grid.len() * 17, np.uint32)
+            geom.L.rh3t_geom_access_table(geom.h, g.access.ctypes.data)
+            g.access = g.access.reshape(-1, 17)
         return g
 
     @classmethod

@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "../../../include/rh3t.h"
+#include "lsbuild.h"
 
 #ifdef _OPENMP
 #include <omp.h>
@@ -304,6 +305,9 @@ struct rh3t_geom {
     std::vector<uint32_t> stencil;
     std::vector<double> s, w, d;
     std::vector<uint32_t> access;
+    // build intermediates: the sorted ghost list and the ghosts with a GhostBC slot
+    std::vector<std::pair<long, long>> found;
+    std::vector<long> heavy;
     std::string err;
 
     bool in_grid(long i, long j) const { return i >= 0 && i < G.nx && j >= 0 && j < G.ny; }
@@ -447,16 +451,16 @@ extern "C" void rh3t_geom_destroy(rh3t_geom* g) { delete g; }
 
 static inline uint64_t pack_ij(long i, long j) { return ((uint64_t)(uint32_t)(int32_t)i << 32) | (uint32_t)(int32_t)j; }
 
-extern "C" int rh3t_geom_build_ghosts(rh3t_geom* g, int32_t n_threads) {
-    if (!g) return RH3T_ERR_INVALID_ARGUMENT;
-#ifdef _OPENMP
-    if (n_threads > 0) omp_set_num_threads(n_threads);
-#else
-    (void)n_threads;
-#endif
+namespace {
+
+const int SOFF[6] = {0, 1, 5, 14, 30, 55}, S2OFF[6] = {0, 1, 17, 98, 354, 979}, WOFF[6] = {0, 1, 9, 36, 100, 225};
+
+// ghost.rs:352-468: discovery, per-ghost geometry, heavy slots
+int build_geometry(rh3t_geom* g) {
     const long nx = g->G.nx, ny = g->G.ny;
     // ---- discovery (ghost.rs:352-376, default offsets ghost.rs:482-493: the radius-4 cross)
-    std::vector<std::pair<long, long>> found;
+    std::vector<std::pair<long, long>>& found = g->found;
+    found.clear();
 #pragma omp parallel
     {
         std::vector<std::pair<long, long>> loc;
@@ -521,27 +525,34 @@ extern "C" int rh3t_geom_build_ghosts(rh3t_geom* g, int32_t n_threads) {
         return RH3T_ERR_GEOMETRY;
     }
     // ---- heavy slots (Wall / Outflow / FarField), in ghost order (ghost.rs:461-468)
-    std::vector<long> heavy;
+    g->heavy.clear();
     for (long k = 0; k < ng; ++k) {
         int kind = (g->boundary[k] == 0 ? g->bc_outer : g->bc_inner)[g->side[k]].kind;
         if (kind == RH3T_BC_WALL || kind == RH3T_BC_OUTFLOW || kind == RH3T_BC_FAR_FIELD) {
-            g->pre[k] = (int32_t)heavy.size();
-            heavy.push_back(k);
+            g->pre[k] = (int32_t)g->heavy.size();
+            g->heavy.push_back(k);
         }
     }
-    const long nh = (long)heavy.size();
+    return RH3T_OK;
+}
+
+// mesh width h and the r = 1..4 smoothness quadratic forms (bc1.rs:62-85)
+double ls_h(const rh3t_geom* g) { return std::sqrt(g->G.dx * g->G.dy); }
+
+// nearest fluid node, the d weights and the E_r stencils of every heavy ghost
+// (bc1.rs:108-160, 1374-1549); tables sized for the least-squares step
+int build_stencils(rh3t_geom* g) {
+    const long ny = g->G.ny;
+    const long nh = (long)g->heavy.size();
     g->nearest.assign(2 * nh, 0); g->stencil.assign(55 * nh, 0u);
     g->s.assign(979 * nh, 0.0); g->w.assign(225 * nh, 0.0); g->d.assign(5 * nh, 0.0);
-    const double h = std::sqrt(g->G.dx * g->G.dy);
-    std::vector<double> M[5];
-    for (int r = 1; r <= 4; ++r) quad_form(r, h, M[r]);
-    static const int SOFF[6] = {0, 1, 5, 14, 30, 55}, S2OFF[6] = {0, 1, 17, 98, 354, 979}, WOFF[6] = {0, 1, 9, 36, 100, 225};
+    const double h = ls_h(g);
     const double dd[5] = {2.0 * ipow(h, 4), 2.0 * ipow(h, 3), 2.0 * ipow(h, 2), 2.0 * h, 0.0};
     const double d4 = 1.0 - dd[0] - dd[1] - dd[2] - dd[3];
     int fit_fail = 0;
 #pragma omp parallel for schedule(dynamic, 8) reduction(| : fit_fail)
     for (long q = 0; q < nh; ++q) {
-        long k = heavy[q];
+        long k = g->heavy[q];
         const double* pr = &g->proj[5 * k];
         long ni, nj;
         g->nearest_node(pr[0], pr[1], ni, nj);
@@ -549,13 +560,36 @@ extern "C" int rh3t_geom_build_ghosts(rh3t_geom* g, int32_t n_threads) {
         for (int r = 0; r < 4; ++r) g->d[5 * q + r] = dd[r];
         g->d[5 * q + 4] = d4;
         for (int r = 0; r <= 4; ++r) {
-            int m = (r + 1) * (r + 1), nt = (r + 1) * (r + 2) / 2;
+            int m = (r + 1) * (r + 1);
             long e[50];
             if (!g->extract(pr, r, e)) { fit_fail = 1; break; }
+            for (int a = 0; a < m; ++a) g->stencil[55 * q + SOFF[r] + a] = (uint32_t)((size_t)e[2 * a] * ny + e[2 * a + 1]);
+        }
+    }
+    if (fit_fail) {
+        g->err = "cannot fit paper substencil inside fluid domain";
+        return RH3T_ERR_STENCIL_FIT;
+    }
+    return RH3T_OK;
+}
+
+// pseudo-inverses, S_r and w_r of every heavy ghost on the host (bc1.rs:120-186)
+void build_ls_host(rh3t_geom* g) {
+    const long ny = g->G.ny;
+    const long nh = (long)g->heavy.size();
+    const double h = ls_h(g);
+    std::vector<double> M[5];
+    for (int r = 1; r <= 4; ++r) quad_form(r, h, M[r]);
+#pragma omp parallel for schedule(dynamic, 8)
+    for (long q = 0; q < nh; ++q) {
+        const double* pr = &g->proj[5 * g->heavy[q]];
+        for (int r = 0; r <= 4; ++r) {
+            int m = (r + 1) * (r + 1), nt = (r + 1) * (r + 2) / 2;
             double A[25 * 15], P[15 * 25];
             for (int a = 0; a < m; ++a) {
-                g->stencil[55 * q + SOFF[r] + a] = (uint32_t)((size_t)e[2 * a] * ny + e[2 * a + 1]);
-                double dx = g->X(e[2 * a]) - pr[0], dy = g->Y(e[2 * a + 1]) - pr[1];
+                const uint32_t l = g->stencil[55 * q + SOFF[r] + a];
+                const long ei = (long)(l / (uint32_t)ny), ej = (long)(l % (uint32_t)ny);
+                double dx = g->X(ei) - pr[0], dy = g->Y(ej) - pr[1];
                 double nor = pr[2] * dx + pr[3] * dy;
                 double tan = -dx * pr[3] + dy * pr[2];
                 int col = 0;
@@ -591,11 +625,13 @@ extern "C" int rh3t_geom_build_ghosts(rh3t_geom* g, int32_t n_threads) {
             }
         }
     }
-    if (fit_fail) {
-        g->err = "cannot fit paper substencil inside fluid domain";
-        return RH3T_ERR_STENCIL_FIT;
-    }
-    // ---- access table (ghost.rs:71-107), radius-4 cross in sorted offset order
+}
+
+// ---- access table (ghost.rs:71-107), radius-4 cross in sorted offset order
+int build_access(rh3t_geom* g) {
+    const long nx = g->G.nx, ny = g->G.ny;
+    const std::vector<std::pair<long, long>>& found = g->found;
+    const long ng = (long)found.size();
     std::unordered_map<uint64_t, uint32_t> lookup;
     lookup.reserve((size_t)ng * 2);
     for (long k = 0; k < ng; ++k) lookup[pack_ij(found[k].first, found[k].second)] = (uint32_t)k;
@@ -628,6 +664,86 @@ extern "C" int rh3t_geom_build_ghosts(rh3t_geom* g, int32_t n_threads) {
     if (miss) {
         g->err = "ghost referenced by a fluid cell is not cached";
         return RH3T_ERR_GEOMETRY;
+    }
+    return RH3T_OK;
+}
+
+} // namespace
+
+extern "C" int rh3t_geom_build_ghosts(rh3t_geom* g, int32_t n_threads) {
+    if (!g) return RH3T_ERR_INVALID_ARGUMENT;
+#ifdef _OPENMP
+    if (n_threads > 0) omp_set_num_threads(n_threads);
+#else
+    (void)n_threads;
+#endif
+    if (int rc = build_geometry(g)) return rc;
+    if (int rc = build_stencils(g)) return rc;
+    build_ls_host(g);
+    return build_access(g);
+}
+
+extern "C" int rh3t_geom_build_ghosts_device(int32_t n, rh3t_geom* const* geoms, int32_t n_threads, int32_t device) {
+    if (n <= 0 || !geoms) return RH3T_ERR_INVALID_ARGUMENT;
+    for (int32_t k = 0; k < n; ++k)
+        if (!geoms[k]) return RH3T_ERR_INVALID_ARGUMENT;
+#ifdef _OPENMP
+    if (n_threads > 0) omp_set_num_threads(n_threads);
+#else
+    (void)n_threads;
+#endif
+    // host phases: one geometry at a time when there are few of them (the
+    // loops inside are parallel), several at once otherwise
+    std::vector<int> rc(n, RH3T_OK);
+    const bool outer = n >= 4;
+#pragma omp parallel for schedule(dynamic, 1) if (outer)
+    for (int32_t k = 0; k < n; ++k) {
+        rh3t_geom* g = geoms[k];
+        int r = build_geometry(g);
+        if (!r) r = build_stencils(g);
+        if (!r) r = build_access(g);
+        rc[k] = r;
+    }
+    for (int32_t k = 0; k < n; ++k)
+        if (rc[k]) return rc[k];
+    // least-squares tables of every heavy ghost of every geometry on the device
+    std::vector<rh3t::LsGrid> grids(n);
+    std::vector<double*> s_out(n), w_out(n);
+    long long total = 0;
+    for (int32_t k = 0; k < n; ++k) {
+        const rh3t_geom* g = geoms[k];
+        rh3t::LsGrid& L = grids[k];
+        L.x0 = g->G.x0; L.y0 = g->G.y0; L.dx = g->G.dx; L.dy = g->G.dy; L.ny = g->G.ny;
+        const double h = ls_h(g);
+        L.s0 = 2.0 * h * h;
+        int off = 0;
+        for (int r = 1; r <= 4; ++r) {
+            std::vector<double> Mr;
+            quad_form(r, h, Mr);
+            std::copy(Mr.begin(), Mr.end(), L.M + off);
+            off += (int)Mr.size();
+        }
+        s_out[k] = geoms[k]->s.data();
+        w_out[k] = geoms[k]->w.data();
+        total += (long long)g->heavy.size();
+    }
+    std::vector<rh3t::LsJob> jobs((size_t)total);
+    std::vector<uint32_t> st((size_t)total * rh3t::LS_STENCIL);
+    long long o = 0;
+    for (int32_t k = 0; k < n; ++k) {
+        const rh3t_geom* g = geoms[k];
+        const long nh = (long)g->heavy.size();
+        for (long q = 0; q < nh; ++q, ++o) {
+            const double* pr = &g->proj[5 * g->heavy[q]];
+            jobs[o] = {pr[0], pr[1], pr[2], pr[3], k, (int32_t)q};
+        }
+        std::copy(g->stencil.begin(), g->stencil.end(), st.begin() + (o - nh) * rh3t::LS_STENCIL);
+    }
+    char err[200] = {0};
+    if (rh3t::ls_tables_device(device, n, grids.data(), total, jobs.data(), st.data(), s_out.data(), w_out.data(),
+                               err, (int)sizeof(err))) {
+        for (int32_t k = 0; k < n; ++k) geoms[k]->err = err;
+        return RH3T_ERR_CUDA;
     }
     return RH3T_OK;
 }

@@ -233,7 +233,7 @@ def adjoint_bench(rh, torch, local, exact, nsteps=200, ckpt=20, n=32):
     reverse sweep)."""
     specs = rh.cases.batch_specs(n, sizes=(121,))
     fields = [rh.cases.batch_field(sp) for sp in specs]
-    grids = [rh.GhostGrid.build(f) for f in fields]
+    grids = rh.GhostGrid.build_many(fields, device=local)
     Js = [rh.cases.SurfacePressure(f, g) for f, g in zip(fields, grids)]
     dev = torch.device(f"cuda:{local}")
 
@@ -287,8 +287,10 @@ def run_batch(args, rh, flops, torch, dist, world, rank, local):
     specs = rh.cases.batch_specs(spec["n"])
     t0 = time.perf_counter()
     fields = [rh.cases.batch_field(sp) for sp in specs]
-    grids = [rh.GhostGrid.build(f) for f in fields]
-    build_s = time.perf_counter() - t0
+    t1 = time.perf_counter()
+    grids = rh.GhostGrid.build_many(fields, device=local)
+    build_s = time.perf_counter() - t1
+    fields_s = t1 - t0
     b = rh.Batch(fields, grids, device=local, exact=args.exact)
     cells = int(sum(int(f.fluid.sum()) for f in fields))
     tune = b.autotune(reps=5)
@@ -385,7 +387,8 @@ def run_batch(args, rh, flops, torch, dist, world, rank, local):
                        "l2": "inputs larger than L2 (state buffers 3 x %.0f MB)" % (
                            6 * 8 * sum((f.grid.nx + 8) * (f.grid.ny + 8) for f in fields) / 1e6),
                        "arithmetic": "no FMA contraction" if args.exact else "FMA contraction",
-                       "ghost_build_s": round(build_s, 3),
+                       "ghost_build_s": round(build_s, 3), "ghost_build": "rh3t_geom_build_ghosts_device",
+                       "field_setup_s": round(fields_s, 3),
                        "tile_shapes": {f"{e['nx']}x{e['ny']}": e["shape"] for e in tune}},
             "instances_per_s": value / cells * b.n,
             "plain_one_at_a_time": {"value": plain_value, "unit": "cell-updates/s", "steps_per_instance": k_plain,

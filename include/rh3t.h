@@ -130,7 +130,8 @@ typedef struct {
 
 /* ------------------------------------------------------------------ */
 /* Host mirror of Field::new + GhostGrid::build (field1.rs:95-136,     */
-/* ghost.rs:50-118, bc1.rs:108-188). Pure host code.                  */
+/* ghost.rs:50-118, bc1.rs:108-188). Host code, apart from the        */
+/* least-squares step of rh3t_geom_build_ghosts_device.               */
 /* ------------------------------------------------------------------ */
 typedef struct rh3t_geom rh3t_geom;
 
@@ -147,6 +148,14 @@ int rh3t_geom_fluid_mask(const rh3t_geom* g, uint8_t* out);
 /* ghost.rs:50-118 GhostGrid::build with ghost.rs:482-493 default offsets;
  * n_threads <= 0 uses all host cores. */
 int rh3t_geom_build_ghosts(rh3t_geom* g, int32_t n_threads);
+/* GhostGrid::build of n geometries (ghost.rs:50-118) with the GhostBC
+ * least-squares tables (bc1.rs:108-188: E_r pseudo-inverses, S_r, w_r)
+ * computed on GPU `device`, one warp per Wall / Outflow / FarField ghost,
+ * all geometries in one pass. Discovery, projection and E_r stencils are
+ * built on the host as by rh3t_geom_build_ghosts; the device tables are
+ * bit-identical to that function's. Returns the first failing geometry's
+ * status (its rh3t_geom_last_error has the text). n_threads as above. */
+int rh3t_geom_build_ghosts_device(int32_t n, rh3t_geom* const* geoms, int32_t n_threads, int32_t device);
 /* view of the built tables (valid until rh3t_geom_destroy) */
 int rh3t_geom_ghost_table(const rh3t_geom* g, rh3t_ghost_table* view);
 /* ghost.rs:71-107 access table, nx*ny*17 u32 (0 for non-fluid cells) */
