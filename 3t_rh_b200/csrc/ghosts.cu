@@ -5,8 +5,9 @@
 // k_ghost_prep, one thread per ghost:
 //   - heavy ghosts (Wall / Outflow / FarField): L, R and lambda at the
 //     nearest fluid node, rotated to the (normal, tangential) frame
-//     (bc1.rs:294-312), written into the ghost's record. Every thread runs
-//     the same six rows, so no lane waits on another's branch;
+//     (bc1.rs:294-312); every thread runs the same six rows, so no lane waits
+//     on another's branch. The 80 doubles of a ghost go through shared
+//     memory and are stored into its record by whole warps (coalesced);
 //   - cheap ghosts (ReflectiveWall, ZerothOrder, Periodic, Constant,
 //     TimeDependent), six threads each, complete.
 // k_ghosts, heavy ghosts on persistent warps, one ghost at a time per warp.
@@ -14,15 +15,16 @@
 // lambda; 10.5 KB) arrives in shared memory by one bulk copy (cp.async.bulk,
 // completion on an mbarrier) issued one ghost ahead, so the table stream
 // overlaps the arithmetic. Per ghost:
-//   2. lanes spread over the 55 stencil nodes of E_0..E_4 (gathered before
-//      the record is awaited): rotate the momentum and project on the six
-//      characteristic fields (bc1.rs:209-219);
+//   1. every lane gathers its E_r stencil nodes (E_0..E_4, 55 nodes);
+//   2. lanes spread over the 55 stencil nodes: rotate the momentum and
+//      project on the six characteristic fields (bc1.rs:209-219);
 //   3. lanes spread over the 55 rows of S_0..S_4: (S_r d_c)_a for all six c,
 //      summed over b in order (bc1.rs:224-229); S_r is stored transposed so
 //      the lanes of one order read consecutive words;
 //   4. lanes (c, r): beta_{c,r} = sum_a d_a (S d)_a and
-//      alpha = d_r / (eps + beta)^q; then a fixed balanced list of
-//      V^(k)_{c,r} = w_{r,k} . d per lane (bc1.rs:221-244);
+//      alpha = d_r / (eps + beta)^q; lanes (r, k), placed on the lanes whose
+//      beta is short: V^(k)_{c,r} = w_{r,k} . d_c for all six c
+//      (bc1.rs:221-244);
 //   5. lanes (k, c): V^(k)_c = sum_r alpha_r / sum(alpha) V_r (bc1.rs:247-252);
 //   6. FarField rows, R products and the Taylor sum on lanes (bc1.rs:829-923);
 //      Wall (two 6x6 LU solves) and Outflow (LODI) on lane 0 (bc1.rs:691-828).
@@ -46,49 +48,17 @@ __constant__ int kStOff[6] = {0, 1, 5, 14, 30, 55};
 __constant__ int kSOff[6] = {0, 1, 17, 98, 354, 979};
 __constant__ int kWOff[6] = {0, 1, 9, 36, 100, 225};
 
-// Step 4 V work lists, one row per lane: (c << 6) | (r << 3) | k, k <= r;
-// 0xffff ends a list. Longest first (LPT) over the 90 dot products of
-// lengths (r+1)^2: 45 terms at most per lane for 1350 in total.
-constexpr int GH_VITEMS = 4;
-__constant__ unsigned short kVItems[32][GH_VITEMS] = {
-    {0x0020, 0x0058, 0x0108, 0xffff},
-    {0x0021, 0x0059, 0x0109, 0xffff},
-    {0x0022, 0x005a, 0x0148, 0xffff},
-    {0x0023, 0x005b, 0x0149, 0xffff},
-    {0x0024, 0x0098, 0x0000, 0xffff},
-    {0x0060, 0x0099, 0x0040, 0xffff},
-    {0x0061, 0x009a, 0x0080, 0xffff},
-    {0x0062, 0x009b, 0x00c0, 0xffff},
-    {0x0063, 0x00d8, 0x0100, 0xffff},
-    {0x0064, 0x00d9, 0x0140, 0xffff},
-    {0x00a0, 0x00da, 0xffff, 0xffff},
-    {0x00a1, 0x00db, 0xffff, 0xffff},
-    {0x00a2, 0x0118, 0xffff, 0xffff},
-    {0x00a3, 0x0119, 0xffff, 0xffff},
-    {0x00a4, 0x011a, 0xffff, 0xffff},
-    {0x00e0, 0x011b, 0xffff, 0xffff},
-    {0x00e1, 0x0158, 0xffff, 0xffff},
-    {0x00e2, 0x0159, 0xffff, 0xffff},
-    {0x00e3, 0x015a, 0xffff, 0xffff},
-    {0x00e4, 0x015b, 0xffff, 0xffff},
-    {0x0120, 0x0010, 0x0110, 0xffff},
-    {0x0121, 0x0011, 0x0111, 0xffff},
-    {0x0122, 0x0012, 0x0112, 0xffff},
-    {0x0123, 0x0050, 0x0150, 0xffff},
-    {0x0124, 0x0051, 0x0151, 0xffff},
-    {0x0160, 0x0052, 0x0152, 0xffff},
-    {0x0161, 0x0090, 0x0008, 0x0088},
-    {0x0162, 0x0091, 0x0009, 0x0089},
-    {0x0163, 0x0092, 0x0048, 0x00c8},
-    {0x0164, 0x00d0, 0x0049, 0x00c9},
-    {0x0018, 0x001a, 0x00d1, 0xffff},
-    {0x0019, 0x001b, 0x00d2, 0xffff},
-};
+// Step 4 V items (r << 3 | k) per lane, 0xff for none: the 15 dot products
+// w_{r,k} . d (all six fields at once), longest on the lanes whose own beta
+// is shortest (lane c * 5 + r computes beta_{c,r}; lanes 30, 31 have none).
+__constant__ unsigned char kVItem[32] = {
+    0x22, 0x1b, 0x00, 0xff, 0xff, 0x23, 0x10, 0xff, 0xff, 0xff, 0x24, 0x11, 0xff, 0xff, 0xff, 0x18,
+    0x12, 0xff, 0xff, 0xff, 0x19, 0x08, 0xff, 0xff, 0xff, 0x1a, 0x09, 0xff, 0xff, 0xff, 0x20, 0x21};
 
 struct GhostWarp {
     double rec[2][GH_REC]; // double-buffered heavy records
-    double D[6][56];       // characteristic data d_c at stencil node a
-    double ACC[6][56];     // (S_r d_c) at stencil row a; later u[5][6] and vinf[6]
+    double D[56][6];       // characteristic data d_c at stencil node a
+    double ACC[56][6];     // (S_r d_c) at stencil row a; later u[5][6] and vinf[6]
     double alpha[6][5];
     double V[6][15];       // [c][r (r + 1) / 2 + k], k <= r
     double v[5][6];        // V^(k)_c
@@ -96,6 +66,7 @@ struct GhostWarp {
 };
 static_assert(sizeof(GhostWarp) % 16 == 0, "records stay 16-byte aligned");
 constexpr int GH_SMEM = GH_WARPS * (int)sizeof(GhostWarp);
+constexpr int GH_LR_R = GH_R - GH_L, GH_LR_LAM = GH_LAM - GH_L;
 
 // ---------------------------------------------------------------- bulk copy
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -180,11 +151,11 @@ __device__ __forceinline__ void r_times(const double* Rc, const double x[6], dou
 
 // Wall (bc1.rs:691-756) and Outflow (bc1.rs:760-828) rows on one lane;
 // fills u[5][6]. Returns false when an ILW system is singular.
-__device__ __noinline__ bool serial_tail(const Inst& I, const GhostRec& Rg, const double* __restrict__ rec,
+__device__ __noinline__ bool serial_tail(const Inst& I, const GhostRec& Rg, const double* LR,
                                          const double (*v)[6], double (*u)[6]) {
     const DevParams& P = I.P;
-    const double* L = rec + GH_L;
-    const double* Rc = rec + GH_R;
+    const double* L = LR;
+    const double* Rc = LR + GH_LR_R;
     if (Rg.kind == BC_WALL) {
         double A0[6][6], rhs0[6];
         for (int i = 0; i < 6; ++i)
@@ -256,36 +227,58 @@ __device__ void cheap_ghost(const Inst& I, const GhostRec& Rg, int c, int stage)
     buf[c * plane + Rg.node] = val;
 }
 
-// blocks [0, nbp): L, R, lambda of one heavy ghost per thread; then cheap ghosts
+// ---------------------------------------------------------------- heavy ghosts
+// L, R and lambda at the nearest fluid node of heavy ghost Rg in its
+// (normal, tangential) frame (bc1.rs:294-312): LR[6c + k] = L[c][k],
+// LR[36 + 6c + i] = R[i][c], LR[72 + c] = lambda_c
+__device__ __forceinline__ void local_lr(const Inst& I, const GhostRec& Rg, const double* __restrict__ buf,
+                                         double* LR, int stride) {
+    const DevParams& P = I.P;
+    double s[6];
+    load6(buf, I.plane, Rg.src, s);
+    const double mom_n = s[1] * Rg.nx + s[2] * Rg.ny;
+    const double mom_t = -s[1] * Rg.ny + s[2] * Rg.nx;
+    const double q6[6] = {s[0], mom_n, mom_t, s[3], s[4], s[5]};
+    const Prim d1 = prim_from_state(q6, P);
+    const Roe q = roe_average(q6[0], d1, q6[0], d1, P);
+    for (int row = 0; row < 6; ++row) {
+        double Lr[6], Rc[6], lam;
+        l_row<0>(row, q, P, Lr);
+        r_col<0>(row, q, P, Rc, lam);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            LR[(6 * row + k) * stride] = Lr[k];
+            LR[(GH_LR_R + 6 * row + k) * stride] = Rc[k];
+        }
+        LR[(GH_LR_LAM + row) * stride] = lam;
+    }
+}
+
+// blocks [0, nbp): L, R, lambda of one heavy ghost per thread, staged in
+// shared memory ([value][thread], stride GH_PREP_THREADS + 1) and stored by
+// whole warps into the records; blocks [nbp, ...): cheap ghosts
+constexpr int GH_PREP_SMEM = GH_LR * (GH_PREP_THREADS + 1) * (int)sizeof(double);
 __global__ void __launch_bounds__(GH_PREP_THREADS) k_ghost_prep(const Inst* __restrict__ insts,
                                                                const GhostRec* __restrict__ heavy, int nh,
                                                                const GhostRec* __restrict__ cheap, int nc,
                                                                double* __restrict__ hrec, int stage, int nbp) {
+    extern __shared__ __align__(16) double prep_smem[];
     if ((int)blockIdx.x < nbp) {
-        const int g = blockIdx.x * GH_PREP_THREADS + threadIdx.x;
-        if (g >= nh) return;
-        const GhostRec Rg = heavy[g];
-        const Inst& I = insts[Rg.inst];
-        if (has_error(I)) return;
-        const DevParams& P = I.P;
-        double s[6];
-        load6(stage_src(I, stage), I.plane, Rg.src, s);
-        const double mom_n = s[1] * Rg.nx + s[2] * Rg.ny;
-        const double mom_t = -s[1] * Rg.ny + s[2] * Rg.nx;
-        const double q6[6] = {s[0], mom_n, mom_t, s[3], s[4], s[5]};
-        const Prim d1 = prim_from_state(q6, P);
-        const Roe q = roe_average(q6[0], d1, q6[0], d1, P);
-        double* r = hrec + (size_t)Rg.heavy * GH_REC;
-        for (int row = 0; row < 6; ++row) {
-            double Lr[6], Rc[6], lam;
-            l_row<0>(row, q, P, Lr);
-            r_col<0>(row, q, P, Rc, lam);
-#pragma unroll
-            for (int k = 0; k < 6; ++k) {
-                r[GH_L + 6 * row + k] = Lr[k];
-                r[GH_R + 6 * row + k] = Rc[k];
-            }
-            r[GH_LAM + row] = lam;
+        constexpr int ST = GH_PREP_THREADS + 1;
+        const int g0 = blockIdx.x * GH_PREP_THREADS, g = g0 + threadIdx.x;
+        if (g < nh) {
+            const GhostRec Rg = heavy[g];
+            const Inst& I = insts[Rg.inst];
+            if (!has_error(I)) local_lr(I, Rg, stage_src(I, stage), prep_smem + threadIdx.x, ST);
+        }
+        __syncthreads();
+        // warp w stores the 80 values of ghosts g0 + 32 w .. g0 + 32 w + 31
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        for (int j = 0; j < 32; ++j) {
+            const int t = 32 * w + j, gj = g0 + t;
+            if (gj >= nh) break;
+            double* r = hrec + (size_t)__ldg(&heavy[gj].heavy) * GH_REC + GH_L;
+            for (int e = lane; e < GH_LR; e += 32) r[e] = prep_smem[e * ST + t];
         }
     } else {
         const int t = (blockIdx.x - nbp) * GH_PREP_THREADS + threadIdx.x;
@@ -298,17 +291,31 @@ __global__ void __launch_bounds__(GH_PREP_THREADS) k_ghost_prep(const Inst* __re
     }
 }
 
-// ---------------------------------------------------------------- heavy ghosts
+__device__ __forceinline__ void load_d6(const double* p, double d[6]) {
+    const double2* q = reinterpret_cast<const double2*>(p);
+    const double2 a = q[0], b = q[1], c = q[2];
+    d[0] = a.x; d[1] = a.y; d[2] = b.x; d[3] = b.y; d[4] = c.x; d[5] = c.y;
+}
+
+__device__ __forceinline__ void store_d6(double* p, const double d[6]) {
+    double2* q = reinterpret_cast<double2*>(p);
+    q[0] = make_double2(d[0], d[1]);
+    q[1] = make_double2(d[2], d[3]);
+    q[2] = make_double2(d[4], d[5]);
+}
+
 // characteristic data of stencil node a from its state (bc1.rs:209-219)
 __device__ __forceinline__ void project_node(GhostWarp& G, const double* __restrict__ L, const double s[6],
                                              double nx, double ny, int a) {
     const double mn = s[1] * nx + s[2] * ny;
     const double mt = -s[1] * ny + s[2] * nx;
     const double u6[6] = {s[0], mn, mt, s[3], s[4], s[5]};
+    double d[6];
 #pragma unroll
     for (int c = 0; c < 6; ++c)
-        G.D[c][a] = L[6 * c + 0] * u6[0] + L[6 * c + 1] * u6[1] + L[6 * c + 2] * u6[2] + L[6 * c + 3] * u6[3] +
-                    L[6 * c + 4] * u6[4] + L[6 * c + 5] * u6[5];
+        d[c] = L[6 * c + 0] * u6[0] + L[6 * c + 1] * u6[1] + L[6 * c + 2] * u6[2] + L[6 * c + 3] * u6[3] +
+               L[6 * c + 4] * u6[4] + L[6 * c + 5] * u6[5];
+    store_d6(G.D[a], d);
 }
 
 // row R of S_r d_c for all six c (S_r transposed in the record)
@@ -320,23 +327,24 @@ __device__ __forceinline__ void acc_row(GhostWarp& G, const double* __restrict__
 #pragma unroll 5
     for (int b = 0; b < m; ++b) {
         const double sv = St[b * m];
+        double d[6];
+        load_d6(G.D[off + b], d);
 #pragma unroll
-        for (int c = 0; c < 6; ++c) acc[c] += sv * G.D[c][off + b];
+        for (int c = 0; c < 6; ++c) acc[c] += sv * d[c];
     }
-#pragma unroll
-    for (int c = 0; c < 6; ++c) G.ACC[c][R] = acc[c];
+    store_d6(G.ACC[R], acc);
 }
 
-__device__ void heavy_ghost(const Inst& I, const GhostRec& Rg, GhostWarp& G, const double* __restrict__ rec,
-                            int lane, int stage, int row1, int row2, const unsigned short vitems[GH_VITEMS],
-                            const double s0[6], const double s1[6]) {
+__device__ __forceinline__ void heavy_ghost(const Inst& I, const GhostRec& Rg, GhostWarp& G,
+                                            const double* __restrict__ rec, int lane, int stage, int row1, int row2,
+                                            unsigned vitem, const double s0[6], const double s1[6]) {
     const DevParams& P = I.P;
     double* buf = const_cast<double*>(stage_src(I, stage));
     const long long plane = I.plane;
     const double nx = Rg.nx, ny = Rg.ny;
-    const double* __restrict__ L = rec + GH_L;
-    const double* __restrict__ Rc = rec + GH_R;
-    const double* __restrict__ lam = rec + GH_LAM;
+    const double* L = rec + GH_L;
+    const double* Rc = rec + GH_R;
+    const double* lam = rec + GH_LAM;
     // 2. characteristic data of the 55 stencil nodes
     project_node(G, L, s0, nx, ny, lane);
     if (lane + 32 < 55) project_node(G, L, s1, nx, ny, lane + 32);
@@ -350,20 +358,25 @@ __device__ void heavy_ghost(const Inst& I, const GhostRec& Rg, GhostWarp& G, con
         const int c = lane / 5, r = lane - 5 * (lane / 5);
         const int m = (r + 1) * (r + 1), off = kStOff[r];
         double beta = 0.0;
-        for (int a = 0; a < m; ++a) beta += G.D[c][off + a] * G.ACC[c][off + a];
+        for (int a = 0; a < m; ++a) beta += G.D[off + a][c] * G.ACC[off + a][c];
         G.alpha[c][r] = rec[GH_D + r] / pow_q(P.eps + beta, P.weno_q);
     }
-    // 4b. V^(k)_{c,r} = w_{r,k} . d
-#pragma unroll
-    for (int q = 0; q < GH_VITEMS; ++q) {
-        const unsigned e = vitems[q];
-        if (e == 0xffffu) break;
-        const int c = (int)(e >> 6), r = (int)((e >> 3) & 7u), k = (int)(e & 7u);
+    // 4b. V^(k)_{c,r} = w_{r,k} . d_c for the six c of item (r, k)
+    if (vitem != 0xffu) {
+        const int r = (int)(vitem >> 3), k = (int)(vitem & 7u);
         const int m = (r + 1) * (r + 1), off = kStOff[r];
         const double* __restrict__ w = rec + GH_W + kWOff[r] + k * m;
-        double v = 0.0;
-        for (int a = 0; a < m; ++a) v += w[a] * G.D[c][off + a];
-        G.V[c][r * (r + 1) / 2 + k] = v;
+        double v[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll 5
+        for (int a = 0; a < m; ++a) {
+            const double wa = w[a];
+            double d[6];
+            load_d6(G.D[off + a], d);
+#pragma unroll
+            for (int c = 0; c < 6; ++c) v[c] += wa * d[c];
+        }
+#pragma unroll
+        for (int c = 0; c < 6; ++c) G.V[c][r * (r + 1) / 2 + k] = v[c];
     }
     __syncwarp();
     // 5. nonlinear weights (bc1.rs:247-252); V^(k)_r = 0 for k > r
@@ -401,7 +414,7 @@ __device__ void heavy_ghost(const Inst& I, const GhostRec& Rg, GhostWarp& G, con
             u[k][i] = acc;
         }
     } else if (lane == 0) {
-        ok = serial_tail(I, Rg, rec, G.v, u);
+        ok = serial_tail(I, Rg, rec + GH_L, G.v, u);
     }
     __syncwarp();
     ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
@@ -435,6 +448,7 @@ __device__ __forceinline__ void gather_stencil(const Inst& I, const double* __re
     if (lane + 32 < 55) load6(buf, I.plane, st[lane + 32], s1);
 }
 
+// warps take the heavy ghosts in turn (record of the next one in flight)
 __global__ void __launch_bounds__(GH_WARPS * 32) k_ghosts(const Inst* __restrict__ insts,
                                                          const GhostRec* __restrict__ heavy, int nh,
                                                          const double* __restrict__ hrec, int stage) {
@@ -443,42 +457,41 @@ __global__ void __launch_bounds__(GH_WARPS * 32) k_ghosts(const Inst* __restrict
     GhostWarp& G = reinterpret_cast<GhostWarp*>(gh_smem)[threadIdx.x >> 5];
     const int stride = gridDim.x * GH_WARPS;
     int g = blockIdx.x * GH_WARPS + (threadIdx.x >> 5);
-    if (g >= nh) return; // warp-uniform
-    // per-lane schedules of steps 3 and 4
-    const int row1 = lane < 25 ? 30 + lane : 14 + (lane - 25);
-    const int row2 = lane < 2 ? 28 + lane
-                     : lane < 11 ? 5 + (lane - 2)
-                     : lane < 15 ? 1 + (lane - 11)
-                     : lane == 15 ? 0
-                     : lane >= 25 ? 21 + (lane - 25) : -1;
-    unsigned short vitems[GH_VITEMS];
-#pragma unroll
-    for (int q = 0; q < GH_VITEMS; ++q) vitems[q] = kVItems[lane][q];
-    if (lane == 0) {
-        mbar_init(&G.bar[0]);
-        mbar_init(&G.bar[1]);
-        mbar_fence_init();
-        bulk_load(G.rec[0], hrec + (size_t)heavy[g].heavy * GH_REC, GH_REC * 8, &G.bar[0]);
-    }
-    __syncwarp();
-    for (int it = 0; g < nh; ++it, g += stride) {
-        const int b = it & 1;
-        const int gn = g + stride;
-        if (lane == 0 && gn < nh)
-            bulk_load(G.rec[b ^ 1], hrec + (size_t)heavy[gn].heavy * GH_REC, GH_REC * 8, &G.bar[b ^ 1]);
-        const GhostRec Rg = heavy[g];
-        const Inst& I = insts[Rg.inst];
-        const bool skip = has_error(I);
-        double s0[6], s1[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-        if (!skip) gather_stencil(I, hrec + (size_t)Rg.heavy * GH_REC, lane, stage, s0, s1);
-        const bool ok = __all_sync(0xffffffffu, mbar_wait(&G.bar[b], (uint32_t)((it >> 1) & 1)));
-        if (!ok) {
-            if (lane == 0) report(I, 1 + 2 * stage, GH_TIMEOUT_CODE, (unsigned)Rg.gid);
-            if (gn < nh) mbar_wait(&G.bar[b ^ 1], (uint32_t)(((it + 1) >> 1) & 1)); // drain the prefetch
-            return;
+    if (g < nh) { // warp-uniform
+        // per-lane schedules of steps 3 and 4
+        const int row1 = lane < 25 ? 30 + lane : 14 + (lane - 25);
+        const int row2 = lane < 2 ? 28 + lane
+                         : lane < 11 ? 5 + (lane - 2)
+                         : lane < 15 ? 1 + (lane - 11)
+                         : lane == 15 ? 0
+                         : lane >= 25 ? 21 + (lane - 25) : -1;
+        const unsigned vitem = kVItem[lane];
+        if (lane == 0) {
+            mbar_init(&G.bar[0]);
+            mbar_init(&G.bar[1]);
+            mbar_fence_init();
+            bulk_load(G.rec[0], hrec + (size_t)heavy[g].heavy * GH_REC, GH_REC * 8, &G.bar[0]);
         }
-        if (!skip) heavy_ghost(I, Rg, G, G.rec[b], lane, stage, row1, row2, vitems, s0, s1);
         __syncwarp();
+        for (int it = 0; g < nh; ++it, g += stride) {
+            const int b = it & 1;
+            const int gn = g + stride;
+            if (lane == 0 && gn < nh)
+                bulk_load(G.rec[b ^ 1], hrec + (size_t)heavy[gn].heavy * GH_REC, GH_REC * 8, &G.bar[b ^ 1]);
+            const GhostRec Rg = heavy[g];
+            const Inst& I = insts[Rg.inst];
+            const bool skip = has_error(I);
+            double s0[6], s1[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+            if (!skip) gather_stencil(I, hrec + (size_t)Rg.heavy * GH_REC, lane, stage, s0, s1);
+            const bool ok = __all_sync(0xffffffffu, mbar_wait(&G.bar[b], (uint32_t)((it >> 1) & 1)));
+            if (!ok) {
+                if (lane == 0) report(I, 1 + 2 * stage, GH_TIMEOUT_CODE, (unsigned)Rg.gid);
+                if (gn < nh) mbar_wait(&G.bar[b ^ 1], (uint32_t)(((it + 1) >> 1) & 1)); // drain the prefetch
+                return;
+            }
+            if (!skip) heavy_ghost(I, Rg, G, G.rec[b], lane, stage, row1, row2, vitem, s0, s1);
+            __syncwarp();
+        }
     }
 }
 
@@ -493,11 +506,12 @@ void launch_ghosts(cudaStream_t s, const Inst* insts, const GhostRec* heavy, int
         int n = 0;
         cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
         cudaFuncSetAttribute(k_ghosts, cudaFuncAttributeMaxDynamicSharedMemorySize, GH_SMEM);
+        cudaFuncSetAttribute(k_ghost_prep, cudaFuncAttributeMaxDynamicSharedMemorySize, GH_PREP_SMEM);
         sm_count[dev] = n > 0 ? n : 1;
     }
     const int nbp = (nh + GH_PREP_THREADS - 1) / GH_PREP_THREADS;
     const int nbc = (nc * 6 + GH_PREP_THREADS - 1) / GH_PREP_THREADS;
-    k_ghost_prep<<<nbp + nbc, GH_PREP_THREADS, 0, s>>>(insts, heavy, nh, cheap, nc, hrec, stage, nbp);
+    k_ghost_prep<<<nbp + nbc, GH_PREP_THREADS, GH_PREP_SMEM, s>>>(insts, heavy, nh, cheap, nc, hrec, stage, nbp);
     if (nh > 0) {
         const int nbh = std::min((nh + GH_WARPS - 1) / GH_WARPS, GH_BLOCKS_PER_SM * sm_count[dev]);
         k_ghosts<<<nbh, GH_WARPS * 32, GH_SMEM, s>>>(insts, heavy, nh, hrec, stage);

@@ -120,6 +120,7 @@ struct Tile {
 // pad (2), written by the ghost preparation kernel.
 constexpr int GH_S = 0, GH_W = 979, GH_D = 1204, GH_ST = 1210;
 constexpr int GH_L = 1238, GH_R = 1274, GH_LAM = 1310;
+constexpr int GH_LR = 80;                        // doubles of the per-stage part at GH_L
 constexpr int GH_REC = 1318;                     // doubles per record (10544 bytes)
 
 constexpr int CELL_TILE = 128;
