@@ -110,8 +110,9 @@ __device__ __forceinline__ void flux_vjp(const double s[6], const Prim& d, const
     prim_vjp(s, P, bu, bv, 0.0, 0.0, 0.0, bp[0], bp[1], bp[2], sb);
 }
 
-// weno.rs:847-886 WENO5: cotangent gb of the result -> ub[5] (added)
-__device__ __forceinline__ void weno5_vjp(const double x[5], double eps, double gb, double ub[5]) {
+// weno.rs:847-886 WENO5: cotangent gb of the result -> ub[5] (added); returns
+// the value itself (formed with the same intermediates)
+__device__ __forceinline__ double weno5_vjp(const double x[5], double eps, double gb, double ub[5]) {
     const double t0 = x[0] - 2.0 * x[1] + x[2], r0 = x[0] - 4.0 * x[1] + 3.0 * x[2];
     const double t1 = x[1] - 2.0 * x[2] + x[3], r1 = x[1] - x[3];
     const double t2 = x[2] - 2.0 * x[3] + x[4], r2 = 3.0 * x[2] - 4.0 * x[3] + x[4];
@@ -142,22 +143,7 @@ __device__ __forceinline__ void weno5_vjp(const double x[5], double eps, double 
     ub[1] += c1 + d1; ub[2] += -2.0 * c1; ub[3] += c1 - d1;
     const double c2 = 13.0 / 6.0 * t2 * bb2, d2 = 0.5 * r2 * bb2;
     ub[2] += c2 + 3.0 * d2; ub[3] += -2.0 * c2 - 4.0 * d2; ub[4] += c2 + d2;
-}
-
-// weno5 of the forward written with reciprocals (the adjoint's recomputation)
-__device__ __forceinline__ double weno5_adj(const double x[5], double eps) {
-    const double c1312 = 13.0 / 12.0;
-    const double t0 = x[0] - 2.0 * x[1] + x[2], r0 = x[0] - 4.0 * x[1] + 3.0 * x[2];
-    const double t1 = x[1] - 2.0 * x[2] + x[3], r1 = x[1] - x[3];
-    const double t2 = x[2] - 2.0 * x[3] + x[4], r2 = 3.0 * x[2] - 4.0 * x[3] + x[4];
-    const double e0 = 1.0 / (eps + (c1312 * t0 * t0 + 0.25 * r0 * r0));
-    const double e1 = 1.0 / (eps + (c1312 * t1 * t1 + 0.25 * r1 * r1));
-    const double e2 = 1.0 / (eps + (c1312 * t2 * t2 + 0.25 * r2 * r2));
-    const double a0 = 0.1 * e0 * e0, a1 = 0.6 * e1 * e1, a2 = 0.3 * e2 * e2;
-    const double p0 = x[0] * K3 - 7.0 / 6.0 * x[1] + 11.0 / 6.0 * x[2];
-    const double p1 = -x[1] * K6 + 5.0 / 6.0 * x[2] + x[3] * K3;
-    const double p2 = x[2] * K3 + 5.0 / 6.0 * x[3] - x[4] * K6;
-    return (a0 * p0 + a1 * p1 + a2 * p2) / (a0 + a1 + a2);
+    return w0 * p0 + w1 * p1 + w2 * p2;
 }
 
 // column c of R and lambda_c (weno.rs:518-545) with reciprocals
@@ -430,20 +416,19 @@ __device__ void adj_flux_tile(const Inst& I, const Tile& t, const double* __rest
             fp[k] = 0.5 * (cf + a * cs);
             fm[k] = 0.5 * (cf - a * cs);
         }
-        {
-            const double xm[5] = {fm[5], fm[4], fm[3], fm[2], fm[1]};
-            S.G[c][f] = weno5_adj(fp, P.eps) + weno5_adj(xm, P.eps);
-        }
+        // g_c = weno5(f+) + weno5(f-) and its cotangent gb = (R^T Fb)_c: both
+        // reconstructions are reversed with the intermediates of their value
         double gb = 0.0;
         for (int i2 = 0; i2 < 6; ++i2) gb += Rc[i2] * S.FB[i2][f];
         double fpb[6] = {0, 0, 0, 0, 0, 0}, fmb[6] = {0, 0, 0, 0, 0, 0};
-        weno5_vjp(fp, P.eps, gb, fpb);
+        double gval = weno5_vjp(fp, P.eps, gb, fpb);
         {
             const double xm[5] = {fm[5], fm[4], fm[3], fm[2], fm[1]};
             double ubm[5] = {0, 0, 0, 0, 0};
-            weno5_vjp(xm, P.eps, gb, ubm);
+            gval += weno5_vjp(xm, P.eps, gb, ubm);
             fmb[5] += ubm[0]; fmb[4] += ubm[1]; fmb[3] += ubm[2]; fmb[2] += ubm[3]; fmb[1] += ubm[4];
         }
+        S.G[c][f] = gval;
         double ab = 0.0, Lb[6] = {0, 0, 0, 0, 0, 0};
         for (int k = 0; k < 6; ++k) {
             const double fbk = 0.5 * (fpb[k] + fmb[k]);
@@ -792,7 +777,22 @@ __global__ void __launch_bounds__(RHS_THREADS) k_adj_cells(const Inst* __restric
 }
 
 // ---------------------------------------------------------------- ghosts
+// Heavy (FarField) ghosts in three launches:
+//   k_adj_ghost_lr    one thread per ghost: L, R and lambda at the nearest
+//                     node of X (bc1.rs:294-312), every thread running the
+//                     same six rows, into the ghost's scratch slot;
+//   k_adj_ghosts      one warp per ghost: the forward pass again (D, S d,
+//                     beta, alpha, V, v) and its reverse down to the
+//                     cotangents of the stencil states (-> Ub), of the
+//                     FarField state and of R (L-bar folded in), which goes
+//                     to the scratch slot; cheap ghosts, one thread each;
+//   k_adj_ghost_tail  one thread per ghost: the Roe base of the nearest
+//                     node's state from R-bar -> Ub at that node.
+// A scratch slot holds AG_SLOT doubles: L (36), R by column (36), lambda (6),
+// pad (2), R-bar (36).
 constexpr int AG_WARPS = 3;
+constexpr int AG_LR_THREADS = 128;
+constexpr int AG_RB = 80;
 __constant__ int kAStOff[6] = {0, 1, 5, 14, 30, 55};
 __constant__ int kASOff[6] = {0, 1, 17, 98, 354, 979};
 __constant__ int kAWOff[6] = {0, 1, 9, 36, 100, 225};
@@ -823,25 +823,70 @@ struct AdjGhostWarp {
 
 __device__ __forceinline__ int aorder(int a) { return a < 1 ? 0 : (a < 5 ? 1 : (a < 14 ? 2 : (a < 30 ? 3 : 4))); }
 
+// the nearest node's state of ghost Rg, rotated to its (n, t) frame, and its Roe state
+__device__ __forceinline__ Roe nearest_roe(const Inst& I, const GhostRec& Rg, const double* __restrict__ X,
+                                           double q6[6]) {
+    double s[6];
+    load6(X, I.plane, Rg.src, s);
+    q6[0] = s[0]; q6[1] = s[1] * Rg.nx + s[2] * Rg.ny; q6[2] = -s[1] * Rg.ny + s[2] * Rg.nx;
+    q6[3] = s[3]; q6[4] = s[4]; q6[5] = s[5];
+    const Prim d1 = prim_from_state(q6, I.P);
+    return roe_average(q6[0], d1, q6[0], d1, I.P);
+}
+
+// L, R, lambda of FarField ghost g into its scratch slot, staged in shared
+// memory ([value][thread]) and stored by whole warps
+constexpr int AG_LR_SMEM = 80 * (AG_LR_THREADS + 1) * (int)sizeof(double);
+__global__ void __launch_bounds__(AG_LR_THREADS) k_adj_ghost_lr(const Inst* __restrict__ insts,
+                                                               const GhostRec* __restrict__ heavy, int nh,
+                                                               const double* __restrict__ Xb,
+                                                               double* __restrict__ slots) {
+    extern __shared__ __align__(16) double lr_smem[];
+    constexpr int ST = AG_LR_THREADS + 1;
+    const int g0 = blockIdx.x * AG_LR_THREADS, g = g0 + threadIdx.x;
+    if (g < nh) {
+        const GhostRec Rg = heavy[g];
+        const Inst& I = insts[Rg.inst];
+        if (!has_error(I) && Rg.kind == BC_FAR_FIELD) {
+            double q6[6];
+            const Roe q = nearest_roe(I, Rg, Xb + I.aoff, q6);
+            double* o = lr_smem + threadIdx.x;
+            for (int row = 0; row < 6; ++row) {
+                double Lr[6], Rcol[6], lm;
+                l_row<0>(row, q, I.P, Lr);
+                r_col<0>(row, q, I.P, Rcol, lm);
+#pragma unroll
+                for (int k = 0; k < 6; ++k) {
+                    o[(6 * row + k) * ST] = Lr[k];
+                    o[(36 + 6 * row + k) * ST] = Rcol[k];
+                }
+                o[(72 + row) * ST] = lm;
+            }
+        }
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int j = 0; j < 32; ++j) {
+        const int t = 32 * w + j, gj = g0 + t;
+        if (gj >= nh) break;
+        double* o = slots + (size_t)gj * AG_SLOT;
+        for (int e = lane; e < 78; e += 32) o[e] = lr_smem[e * ST + t];
+    }
+}
+
 // one heavy (FarField) ghost per warp; gb from W at the ghost node
 __device__ void ghost_vjp_warp(const Inst& I, const GhostRec& Rg, const double* __restrict__ rec,
                                const double* __restrict__ X, const double* __restrict__ W, double* __restrict__ Ub,
-                               double* __restrict__ pbar_k, AdjGhostWarp& G, int lane) {
+                               double* __restrict__ pbar_k, double* __restrict__ slot, AdjGhostWarp& G, int lane) {
     const DevParams& P = I.P;
     const long long plane = I.plane;
     const double nx = Rg.nx, ny = Rg.ny;
-    // L, R, lambda at the nearest node of X (bc1.rs:294-312)
-    if (lane < 6) {
-        double s[6];
-        load6(X, plane, Rg.src, s);
-        const double q6[6] = {s[0], s[1] * nx + s[2] * ny, -s[1] * ny + s[2] * nx, s[3], s[4], s[5]};
-        const Prim d1 = prim_from_state(q6, P);
-        const Roe q = roe_average(q6[0], d1, q6[0], d1, P);
-        double Lr[6], Rcol[6], lm;
-        l_row<0>(lane, q, P, Lr);
-        r_col<0>(lane, q, P, Rcol, lm);
-        for (int k = 0; k < 6; ++k) { G.L[6 * lane + k] = Lr[k]; G.R[6 * lane + k] = Rcol[k]; }
-        G.lam[lane] = lm;
+    // L, R, lambda at the nearest node of X (k_adj_ghost_lr)
+    for (int e = lane; e < 78; e += 32) {
+        const double v = slot[e];
+        if (e < 36) G.L[e] = v;
+        else if (e < 72) G.R[e - 36] = v;
+        else G.lam[e - 72] = v;
     }
     __syncwarp();
     const double* L = G.L;    // L[c][j] = L[6c + j]
@@ -1038,23 +1083,36 @@ __device__ void ghost_vjp_warp(const Inst& I, const GhostRec& Rg, const double* 
         G.Rb[c][i] -= acc;
     }
     __syncwarp();
-    if (lane == 0) {
-        double s[6];
-        load6(X, plane, Rg.src, s);
-        const double q6[6] = {s[0], s[1] * nx + s[2] * ny, -s[1] * ny + s[2] * nx, s[3], s[4], s[5]};
-        const Prim d1 = prim_from_state(q6, P);
-        const Roe q = roe_average(q6[0], d1, q6[0], d1, P);
-        const double base[5] = {q.u, q.v, q.ee, q.ei, q.er};
-        const double lamb[6] = {0, 0, 0, 0, 0, 0};
-        double bb[5] = {0, 0, 0, 0, 0};
-        r_base_vjp<0>(base, P, G.Rb, lamb, bb);
-        double ga[6] = {0, 0, 0, 0, 0, 0}, gb2[6] = {0, 0, 0, 0, 0, 0};
-        roe_vjp(q6, q6, P, bb, ga, gb2);
-        double gr[6];
-        for (int c = 0; c < 6; ++c) gr[c] = ga[c] + gb2[c];
-        const double sb[6] = {gr[0], gr[1] * nx - gr[2] * ny, gr[1] * ny + gr[2] * nx, gr[3], gr[4], gr[5]};
-        atomic_add6(Ub, plane, Rg.src, sb);
-    }
+    // R-bar to the scratch slot (k_adj_ghost_tail)
+    for (int e = lane; e < 36; e += 32) slot[AG_RB + e] = G.Rb[e / 6][e - 6 * (e / 6)];
+}
+
+// the Roe base of the nearest node of FarField ghost g from its R-bar -> Ub
+__global__ void __launch_bounds__(128) k_adj_ghost_tail(const Inst* __restrict__ insts,
+                                                        const GhostRec* __restrict__ heavy, int nh,
+                                                        const double* __restrict__ Xb,
+                                                        const double* __restrict__ slots, double* __restrict__ Ubb) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= nh) return;
+    const GhostRec Rg = heavy[g];
+    const Inst& I = insts[Rg.inst];
+    if (has_error(I) || Rg.kind != BC_FAR_FIELD) return;
+    double q6[6];
+    const Roe q = nearest_roe(I, Rg, Xb + I.aoff, q6);
+    const double* o = slots + (size_t)g * AG_SLOT + AG_RB;
+    double Rb[6][6];
+    for (int e = 0; e < 36; ++e) Rb[e / 6][e - 6 * (e / 6)] = o[e];
+    const double base[5] = {q.u, q.v, q.ee, q.ei, q.er};
+    const double lamb[6] = {0, 0, 0, 0, 0, 0};
+    double bb[5] = {0, 0, 0, 0, 0};
+    r_base_vjp<0>(base, I.P, Rb, lamb, bb);
+    double ga[6] = {0, 0, 0, 0, 0, 0}, gb2[6] = {0, 0, 0, 0, 0, 0};
+    roe_vjp(q6, q6, I.P, bb, ga, gb2);
+    double gr[6];
+    for (int c = 0; c < 6; ++c) gr[c] = ga[c] + gb2[c];
+    const double nx = Rg.nx, ny = Rg.ny;
+    const double sb[6] = {gr[0], gr[1] * nx - gr[2] * ny, gr[1] * ny + gr[2] * nx, gr[3], gr[4], gr[5]};
+    atomic_add6(Ubb + I.aoff, I.plane, Rg.src, sb);
 }
 
 __global__ void __launch_bounds__(AG_WARPS * 32) k_adj_ghosts(const Inst* __restrict__ insts,
@@ -1064,7 +1122,7 @@ __global__ void __launch_bounds__(AG_WARPS * 32) k_adj_ghosts(const Inst* __rest
                                                              const double* __restrict__ Xb,
                                                              const double* __restrict__ Wb,
                                                              double* __restrict__ Ubb, double* __restrict__ pbar,
-                                                             int nbh) {
+                                                             double* __restrict__ slots, int nbh) {
     __shared__ AdjGhostWarp G[AG_WARPS];
     const int lane = threadIdx.x & 31;
     if ((int)blockIdx.x < nbh) {
@@ -1074,7 +1132,7 @@ __global__ void __launch_bounds__(AG_WARPS * 32) k_adj_ghosts(const Inst* __rest
         const Inst& I = insts[Rg.inst];
         if (has_error(I) || Rg.kind != BC_FAR_FIELD) return;
         ghost_vjp_warp(I, Rg, hrec + (size_t)Rg.heavy * GH_REC, Xb + I.aoff, Wb + I.aoff, Ubb + I.aoff,
-                       pbar + 8 * Rg.inst, G[threadIdx.x >> 5], lane);
+                       pbar + 8 * Rg.inst, slots + (size_t)g * AG_SLOT, G[threadIdx.x >> 5], lane);
     } else {
         const int g = (blockIdx.x - nbh) * (AG_WARPS * 32) + threadIdx.x;
         if (g >= nc) return;
@@ -1116,25 +1174,31 @@ __global__ void k_adj_fluid(const Inst* __restrict__ insts, int k0, const double
 void launch_adj_l(cudaStream_t s, const Inst* insts, int k0, int n, long long max_cells, const Tile* tx, int ntx,
                   const Tile* ty, int nty, const Tile* tr, int ntr, const GhostRec* heavy, int nh,
                   const GhostRec* cheap, int nc, const double* hrec, const double* X, const double* rbar, double* W,
-                  double* Ub, double* pbar) {
+                  double* Ub, double* pbar, double* slots) {
     if (n <= 0) return;
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(k_adj_cells, cudaFuncAttributeMaxDynamicSharedMemorySize, ADJ_CELL_SMEM);
         cudaFuncSetAttribute(k_adj_flux, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(AdjFluxShared));
+        cudaFuncSetAttribute(k_adj_ghost_lr, cudaFuncAttributeMaxDynamicSharedMemorySize, AG_LR_SMEM);
         attr = true;
     }
+    if (nh > 0)
+        k_adj_ghost_lr<<<(nh + AG_LR_THREADS - 1) / AG_LR_THREADS, AG_LR_THREADS, AG_LR_SMEM, s>>>(insts, heavy, nh,
+                                                                                                  X, slots);
     const unsigned cb = (unsigned)((max_cells + 127) / 128);
     if (ntx + nty > 0)
         k_adj_flux<<<ntx + nty, FLUX_THREADS, sizeof(AdjFluxShared), s>>>(insts, tx, ntx, ty, nty, X, rbar, W);
     if (ntr > 0) k_adj_cells<<<ntr, RHS_THREADS, ADJ_CELL_SMEM, s>>>(insts, tr, ntr, X, rbar, W, pbar);
     const int nbh = (nh + AG_WARPS - 1) / AG_WARPS, nbc = (nc + AG_WARPS * 32 - 1) / (AG_WARPS * 32);
     if (nbh + nbc > 0)
-        k_adj_ghosts<<<nbh + nbc, AG_WARPS * 32, 0, s>>>(insts, heavy, nh, cheap, nc, hrec, X, W, Ub, pbar, nbh);
+        k_adj_ghosts<<<nbh + nbc, AG_WARPS * 32, 0, s>>>(insts, heavy, nh, cheap, nc, hrec, X, W, Ub, pbar, slots,
+                                                          nbh);
+    if (nh > 0) k_adj_ghost_tail<<<(nh + 127) / 128, 128, 0, s>>>(insts, heavy, nh, X, slots, Ub);
     k_adj_fluid<<<dim3(cb, n), 128, 0, s>>>(insts, k0, W, Ub);
 }
 
-int adj_l_launches(int nh, int nc) { return 3 + (nh + nc > 0 ? 1 : 0); }
+int adj_l_launches(int nh, int nc) { return 3 + (nh + nc > 0 ? 1 : 0) + (nh > 0 ? 2 : 0); }
 
 // ---------------------------------------------------------------- RK3 step plumbing
 // copy the 6 planes of stage buffer `which` (0 U, 1 A, 2 B) of instances

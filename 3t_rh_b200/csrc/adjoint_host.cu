@@ -36,14 +36,15 @@ struct AdjBuffers {
     double* pbar = nullptr;     // n_inst x 8
     double* dtbar = nullptr;    // n_inst
     unsigned long long* argmin = nullptr; // n_inst: the dt-minimising cell
+    double* gslots = nullptr;   // AG_SLOT doubles per heavy ghost (ghost vjp scratch)
 };
 
 namespace rh3t {
 void adj_free(rh3t_ctx* c) {
     AdjBuffers* a = c->adj;
     if (!a) return;
-    void* ptrs[] = {a->ckpt, a->ckpt_sc, a->seg,  a->seg_sc, a->Y,     a->U0,
-                    a->U1,   a->U2,      a->W,    a->rbar,   a->pbar, a->dtbar, a->argmin};
+    void* ptrs[] = {a->ckpt, a->ckpt_sc, a->seg,  a->seg_sc, a->Y,     a->U0,    a->U1,
+                    a->U2,   a->W,       a->rbar, a->pbar,   a->dtbar, a->argmin, a->gslots};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete a;
@@ -84,6 +85,7 @@ int ensure_work(rh3t_ctx* c) {
     CK(c, cudaMalloc(&a->pbar, (size_t)c->n_inst * 8 * sizeof(double)));
     CK(c, cudaMalloc(&a->dtbar, (size_t)c->n_inst * sizeof(double)));
     CK(c, cudaMalloc(&a->argmin, (size_t)c->n_inst * sizeof(unsigned long long)));
+    CK(c, cudaMalloc(&a->gslots, (size_t)std::max(c->n_gheavy, 1) * AG_SLOT * sizeof(double)));
     return RH3T_OK;
 }
 
@@ -100,7 +102,7 @@ void enqueue_vjp_l(rh3t_ctx* c, const double* X, const double* rbar, double* Ub)
     int nh, nc;
     ghost_ranges(c, nh, nc);
     launch_adj_l(c->stream, c->d_inst, 0, c->n_inst, c->max_cells, c->d_tx, c->ntx, c->d_ty, c->nty, c->d_tr, c->ntr,
-                 c->d_gpart, nh, c->d_gpart + c->n_gheavy, nc, c->d_hrec, X, rbar, a->W, Ub, a->pbar);
+                 c->d_gpart, nh, c->d_gpart + c->n_gheavy, nc, c->d_hrec, X, rbar, a->W, Ub, a->pbar, a->gslots);
     c->launches += adj_l_launches(nh, nc);
 }
 

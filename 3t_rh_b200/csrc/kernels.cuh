@@ -23,11 +23,13 @@ void launch_ghost_values(cudaStream_t s, const Inst* insts, const GhostRec* recs
 void launch_dfma(cudaStream_t s, int blocks, double* out, int iters);
 // adjoint (adjoint.cu): plane sets are batch-wide arrays of 6 padded planes
 // per instance at Inst::aoff
-// tx, ty, tr: the face and RHS tiles of instances [k0, k0 + n)
+// tx, ty, tr: the face and RHS tiles of instances [k0, k0 + n); slots:
+// AG_SLOT doubles of scratch per heavy ghost
+constexpr int AG_SLOT = 120;
 void launch_adj_l(cudaStream_t s, const Inst* insts, int k0, int n, long long max_cells, const Tile* tx, int ntx,
                   const Tile* ty, int nty, const Tile* tr, int ntr, const GhostRec* heavy, int nh,
                   const GhostRec* cheap, int nc, const double* hrec, const double* X, const double* rbar, double* W,
-                  double* Ub, double* pbar);
+                  double* Ub, double* pbar, double* slots);
 int adj_l_launches(int nh, int nc);
 void launch_adj_copy(cudaStream_t s, const Inst* insts, int k0, int n, long long max_plane, int which, double* set,
                      int dir);
