@@ -203,6 +203,24 @@ __device__ __forceinline__ void roe_vjp(const double sa[6], const double sb_[6],
     prim_vjp(sb_, P, pb[0], pb[1], pb[2], pb[3], pb[4], 0.0, 0.0, 0.0, gb);
 }
 
+// One side of roe_vjp: the cotangent of point 3 (side 0, sa) or point 2
+// (side 1, sb_) only, added to g
+__device__ __forceinline__ void roe_vjp_side(const double sa[6], const double sb_[6], const DevParams& P,
+                                             const double bb[5], int side, double g[6]) {
+    const Prim da = prim_from_state(sa, P), db = prim_from_state(sb_, P);
+    const double ra = sqrt(sa[0]), rb = sqrt(sb_[0]), irs = 1.0 / (ra + rb);
+    const double xa[5] = {da.u, da.v, da.e_e, da.e_i, da.e_r}, xb[5] = {db.u, db.v, db.e_e, db.e_i, db.e_r};
+    const double rs_self = side == 0 ? ra : rb;
+    double br = 0.0, pp[5];
+    for (int k = 0; k < 5; ++k) {
+        const double base = (xa[k] * ra + xb[k] * rb) * irs;
+        pp[k] = bb[k] * rs_self * irs;
+        br += bb[k] * ((side == 0 ? xa[k] : xb[k]) - base) * irs;
+    }
+    g[0] += br / (2.0 * rs_self);
+    prim_vjp(side == 0 ? sa : sb_, P, pp[0], pp[1], pp[2], pp[3], pp[4], 0.0, 0.0, 0.0, g);
+}
+
 // Cotangents of R (Rb[c][i] = dJ/dR[i][c], weno.rs:518-545) and of the
 // eigenvalues -> cotangents of the Roe base (u, v, e_e, e_i, e_r), added.
 // R is written in u, v, w2 = u^2 + v^2, cs = sqrt(cs2) and the e_k.
@@ -346,52 +364,54 @@ __device__ void adj_flux_tile(const Inst& I, const Tile& t, const double* __rest
     const int cols = 1 << t.lg, rows = FLUX_FACES >> t.lg;
     const int np = DIR == 0 ? (rows + 5) * cols : rows * (cols + 5);
     const double sc = DIR == 0 ? 1.0 / I.dx : 1.0 / I.dy;
-    // ---- 1. staging
-    for (int w = threadIdx.x; w < np + FLUX_FACES; w += blockDim.x) {
-        if (w < np) {
-            const int p = w;
-            int pi, pj;
-            if (DIR == 0) { pi = t.i - 3 + (p >> t.lg); pj = t.j0 + (p & (cols - 1)); }
-            else { const int r = p / (cols + 5); pi = t.i + r; pj = t.j0 - 3 + (p - r * (cols + 5)); }
-            double s[6] = {1.0, 0.0, 0.0, 1.0, 1.0, 1.0};
-            if (pi >= -RH3T_PAD && pi < nx + RH3T_PAD && pj >= -RH3T_PAD && pj < ny + RH3T_PAD)
-                load6(X, plane, node_of(I, pi, pj), s);
-            const Prim d = prim_from_state(s, P);
-            double f[6];
-            phys_flux<DIR>(s, d, f);
-            for (int k = 0; k < 3; ++k) {
-                S.U[k][p] = make_double2(s[2 * k], s[2 * k + 1]);
-                S.F[k][p] = make_double2(f[2 * k], f[2 * k + 1]);
-            }
-        } else {
-            const int f = w - np;
-            int i, j, p0, ps;
-            adj_face_index<DIR>(t, f, i, j, p0, ps);
-            bool valid = DIR == 0 ? (i <= nx && j < ny) : (i < nx && j <= ny);
-            long long n3 = 0, n2 = 0;
-            if (valid) {
-                n3 = node_of(I, i, j);
-                n2 = DIR == 0 ? node_of(I, i - 1, j) : node_of(I, i, j - 1);
-                valid = (I.mask[n3] | I.mask[n2]) != 0;
-            }
-            S.act[f] = valid ? 1 : 0;
-            if (!valid) continue;
-            double s3[6], s2[6];
-            load6(X, plane, n3, s3);
-            load6(X, plane, n2, s2);
-            const Prim d3 = prim_from_state(s3, P), d2 = prim_from_state(s2, P);
-            const Roe q = roe_average(s3[0], d3, s2[0], d2, P);
-            const double qv[15] = {q.u,  q.v,  q.w2, q.ee, q.ei, q.er,  q.cs2,       q.cs,
-                                   q.he, q.hi, q.hr, q.b,  q.den, 1.0 / q.cs2, 1.0 / q.b};
-            for (int k = 0; k < 15; ++k) S.Q[k][f] = qv[k];
-            const bool in3 = DIR == 0 ? (i < nx) : (j < ny);
-            const bool in2 = DIR == 0 ? (i >= 1) : (j >= 1);
-            for (int c = 0; c < 6; ++c) {
-                const double r3 = in3 && I.mask[n3] ? rbar[c * plane + n3] : 0.0;
-                const double r2 = in2 && I.mask[n2] ? rbar[c * plane + n2] : 0.0;
-                S.FB[c][f] = (r3 - r2) * sc;
-            }
+    // ---- 1a. points of the tile: state, physical flux, primitives, mask and
+    // rbar (fluid nodes of the grid, else 0); primitives, rbar and mask live in
+    // the L rows' space until step 2
+    double* const stage_tmp = &S.LS[0][0][0];
+    double(*PR)[FLUX_NPT] = reinterpret_cast<double(*)[FLUX_NPT]>(stage_tmp);
+    double(*RB)[FLUX_NPT] = reinterpret_cast<double(*)[FLUX_NPT]>(stage_tmp + 8 * FLUX_NPT);
+    unsigned char* MK = reinterpret_cast<unsigned char*>(stage_tmp + 14 * FLUX_NPT);
+    for (int p = threadIdx.x; p < np; p += blockDim.x) {
+        int pi, pj;
+        if (DIR == 0) { pi = t.i - 3 + (p >> t.lg); pj = t.j0 + (p & (cols - 1)); }
+        else { const int r = p / (cols + 5); pi = t.i + r; pj = t.j0 - 3 + (p - r * (cols + 5)); }
+        double s[6] = {1.0, 0.0, 0.0, 1.0, 1.0, 1.0};
+        unsigned char mk = 0;
+        long long n = 0;
+        if (pi >= -RH3T_PAD && pi < nx + RH3T_PAD && pj >= -RH3T_PAD && pj < ny + RH3T_PAD) {
+            n = node_of(I, pi, pj);
+            load6(X, plane, n, s);
+            mk = I.mask[n];
         }
+        const Prim d = prim_from_state(s, P);
+        double f[6];
+        phys_flux<DIR>(s, d, f);
+        for (int k = 0; k < 3; ++k) {
+            S.U[k][p] = make_double2(s[2 * k], s[2 * k + 1]);
+            S.F[k][p] = make_double2(f[2 * k], f[2 * k + 1]);
+        }
+        PR[0][p] = d.u; PR[1][p] = d.v; PR[2][p] = d.e_e; PR[3][p] = d.e_i; PR[4][p] = d.e_r;
+        PR[5][p] = d.pe; PR[6][p] = d.pi; PR[7][p] = d.pr;
+        const bool in = mk && pi >= 0 && pi < nx && pj >= 0 && pj < ny;
+        for (int c = 0; c < 6; ++c) RB[c][p] = in ? rbar[c * plane + n] : 0.0;
+        MK[p] = mk;
+    }
+    __syncthreads();
+    // ---- 1b. faces: Roe state of points 3 and 2, flux cotangent Fb
+    for (int f = threadIdx.x; f < FLUX_FACES; f += blockDim.x) {
+        int i, j, p0, ps;
+        adj_face_index<DIR>(t, f, i, j, p0, ps);
+        const int p3 = p0 + 3 * ps, p2 = p0 + 2 * ps;
+        const bool valid = (DIR == 0 ? (i <= nx && j < ny) : (i < nx && j <= ny)) && (MK[p3] | MK[p2]) != 0;
+        S.act[f] = valid ? 1 : 0;
+        if (!valid) continue;
+        const Prim d3 = {PR[0][p3], PR[1][p3], PR[2][p3], PR[3][p3], PR[4][p3], PR[5][p3], PR[6][p3], PR[7][p3]};
+        const Prim d2 = {PR[0][p2], PR[1][p2], PR[2][p2], PR[3][p2], PR[4][p2], PR[5][p2], PR[6][p2], PR[7][p2]};
+        const Roe q = roe_average(S.U[0][p3].x, d3, S.U[0][p2].x, d2, P);
+        const double qv[15] = {q.u,  q.v,  q.w2, q.ee, q.ei, q.er,  q.cs2,       q.cs,
+                               q.he, q.hi, q.hr, q.b,  q.den, 1.0 / q.cs2, 1.0 / q.b};
+        for (int k = 0; k < 15; ++k) S.Q[k][f] = qv[k];
+        for (int c = 0; c < 6; ++c) S.FB[c][f] = (RB[c][p3] - RB[c][p2]) * sc;
     }
     __syncthreads();
     // ---- 2. warp c: field c of faces lane and lane + 32
@@ -493,8 +513,9 @@ __device__ void adj_flux_tile(const Inst& I, const Tile& t, const double* __rest
                     VF[h][m] = b;
                 }
             }
-        __syncthreads(); // LB, WB, G and LAMB are read: reuse them
+        __syncthreads(); // LB, WB, FK, G and LAMB are read: reuse them
         if (on) {
+            if (part == 0) for (int m = 0; m < 5; ++m) S.FK[0][m][f] = bb[m];
             if (part == 1) for (int m = 0; m < 5; ++m) S.G[m][f] = bb[m];
             if (part == 2) for (int m = 0; m < 5; ++m) S.LAMB[m][f] = bb[m];
             for (int h = 0; h < 2; ++h)
@@ -504,17 +525,22 @@ __device__ void adj_flux_tile(const Inst& I, const Tile& t, const double* __rest
                 }
         }
         __syncthreads();
-        if (on && part == 0) {
-            for (int m = 0; m < 5; ++m) bb[m] += S.G[m][f] + S.LAMB[m][f];
+        if (on && part < 2) { // the Roe average's vjp: point 3 on part 0, point 2 on part 1
+            for (int m = 0; m < 5; ++m) bb[m] = S.FK[0][m][f] + (S.G[m][f] + S.LAMB[m][f]);
             int i, j, p0, ps;
             adj_face_index<DIR>(t, f, i, j, p0, ps);
             double u3[6], u2[6], F_[6];
             adj_point(S, p0 + 3 * ps, u3, F_);
             adj_point(S, p0 + 2 * ps, u2, F_);
-            double g3[6] = {0, 0, 0, 0, 0, 0}, g2[6] = {0, 0, 0, 0, 0, 0};
-            roe_vjp(u3, u2, P, bb, g3, g2);
-            atomic_add6(W, plane, node_of(I, i, j), g3);
-            atomic_add6(W, plane, DIR == 0 ? node_of(I, i - 1, j) : node_of(I, i, j - 1), g2);
+            double g[6] = {0, 0, 0, 0, 0, 0};
+            roe_vjp_side(u3, u2, P, bb, part, g);
+            atomic_add6(W, plane, part == 0 ? node_of(I, i, j) : (DIR == 0 ? node_of(I, i - 1, j) : node_of(I, i, j - 1)),
+                        g);
+        }
+        if (on && part == 2) {
+            int i, j, p0, ps;
+            adj_face_index<DIR>(t, f, i, j, p0, ps);
+            double F_[6];
             if (I.diffusion) { // diffusion.rs:27-50: rhs += -(b - a) cx per face pair, cx = -1 / ds^2
                 const double cx = DIR == 0 ? -1.0 / (I.dx * I.dx) : -1.0 / (I.dy * I.dy);
                 const double Db[3] = {S.FB[3][f] / sc * cx, S.FB[4][f] / sc * cx, S.FB[5][f] / sc * cx};

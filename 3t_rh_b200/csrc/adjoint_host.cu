@@ -13,7 +13,9 @@
 //   dt = cfl dt_cfl(u0): U0 += cfl dtbar d(local dt)/du at the minimising cell,
 //   with dtbar = <r2, 2Y/3> + <r1, U2/4> + <r0, U1>;
 // and U0 is the next Y. Memory: (n_steps / ckpt_every) states plus
-// ckpt_every x (3 stage states + 3 rhs) plane sets.
+// ckpt_every x (3 stage states + 3 rhs) plane sets. The forward run records
+// its last segment as it goes, so the first segment of the reverse sweep is
+// not recomputed.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -27,6 +29,7 @@ using namespace rh3t;
 
 struct AdjBuffers {
     int ckpt_every = 0, nsteps = 0, n_ckpt = 0;
+    bool last_recorded = false; // seg holds the forward run's last segment
     double cfl = 0.05;
     double* ckpt = nullptr;     // n_ckpt plane sets (state U at segment starts)
     DevScalars* ckpt_sc = nullptr; // n_ckpt x n_inst scalars at segment starts
@@ -182,6 +185,7 @@ extern "C" int rh3t_adjoint_forward(rh3t_ctx* c, int32_t nsteps, double cfl_fact
         CK(c, cudaMalloc(&a->seg, (size_t)ckpt_every * 6 * np * sizeof(double)));
         CK(c, cudaMalloc(&a->seg_sc, (size_t)ckpt_every * ni * sizeof(DevScalars)));
     }
+    a->last_recorded = false;
     a->n_ckpt = n_ckpt;
     a->ckpt_every = ckpt_every;
     a->nsteps = nsteps;
@@ -197,10 +201,23 @@ extern "C" int rh3t_adjoint_forward(rh3t_ctx* c, int32_t nsteps, double cfl_fact
                               s));
         c->launches += 1;
         const int len = std::min(ckpt_every, nsteps - done);
-        rc = rh3t_advance(c, len, cfl_factor, INFINITY, 1);
-        if (rc) return rc;
+        if (q + 1 < n_ckpt) {
+            rc = rh3t_advance(c, len, cfl_factor, INFINITY, 1);
+            if (rc) return rc;
+        } else {
+            // the last segment with its record (stage states, rhs, scalars)
+            for (int j = 0; j < len; ++j) {
+                enqueue_recorded_step(c, a->seg + (size_t)j * 6 * np);
+                CK(c, cudaMemcpyAsync(a->seg_sc + (size_t)j * ni, c->d_sc, ni * sizeof(DevScalars),
+                                      cudaMemcpyDeviceToDevice, s));
+            }
+            CK(c, cudaGetLastError());
+            rc = fetch_status(c);
+            if (rc) return rc;
+        }
         done += len;
     }
+    a->last_recorded = true;
     return RH3T_OK;
 }
 
@@ -226,12 +243,16 @@ extern "C" int rh3t_adjoint_backward(rh3t_ctx* c, const double* dJ_du, double* d
     launch_adj_copy(s, c->d_inst, 0, c->n_inst, mp, 0, final_state, 0);
     for (int q = a->n_ckpt - 1; q >= 0; --q) {
         const int len = std::min(a->ckpt_every, a->nsteps - q * a->ckpt_every);
-        // recompute the segment with its record
-        launch_adj_copy(s, c->d_inst, 0, c->n_inst, mp, 0, a->ckpt + (size_t)q * np, 1);
-        CK(c, cudaMemcpyAsync(c->d_sc, a->ckpt_sc + (size_t)q * ni, ni * sizeof(DevScalars), cudaMemcpyDeviceToDevice,
-                              s));
-        c->launches += 1;
-        for (int j = 0; j < len; ++j) {
+        // recompute the segment with its record (the last one is recorded already)
+        const bool have = q == a->n_ckpt - 1 && a->last_recorded;
+        a->last_recorded = false;
+        if (!have) {
+            launch_adj_copy(s, c->d_inst, 0, c->n_inst, mp, 0, a->ckpt + (size_t)q * np, 1);
+            CK(c, cudaMemcpyAsync(c->d_sc, a->ckpt_sc + (size_t)q * ni, ni * sizeof(DevScalars),
+                                  cudaMemcpyDeviceToDevice, s));
+            c->launches += 1;
+        }
+        for (int j = 0; j < len && !have; ++j) {
             double* rec = a->seg + (size_t)j * 6 * np;
             // the step's scalars are those after its dt: record them after the step
             enqueue_recorded_step(c, rec);
