@@ -317,19 +317,24 @@ __device__ __forceinline__ void atomic_add6(double* W, long long plane, long lon
 //      sum_c w-bar_ck L_c and sum_c f-bar_ck L_c;
 //   3b. one thread per point: the sums of 3a over the faces that use it, the
 //      physical flux's vjp -> W (atomic).
+// per-face rows are padded to FLUX_FACES + 1 doubles: the three threads of a
+// face in step 3a read different rows at the same face and land in different
+// banks
+constexpr int AFP = FLUX_FACES + 1;
 struct AdjFluxShared {
     double2 U[3][FLUX_NPT];
     double2 F[3][FLUX_NPT];
-    double Q[15][FLUX_FACES];     // Roe state u v w2 ee ei er cs2 cs he hi hr b den, 1/cs2, 1/b
-    double FB[6][FLUX_FACES];     // face flux cotangent
-    double G[6][FLUX_FACES];      // g_c
-    double LAMB[6][FLUX_FACES];   // lambda-bar_c
-    double LS[6][6][FLUX_FACES];  // L row c
-    double LB[6][6][FLUX_FACES];  // L-bar row c
-    double WB[6][6][FLUX_FACES];  // w-bar [c][k]
-    double FK[6][6][FLUX_FACES];  // f-bar [c][k]
+    double Q[15][AFP];     // Roe state u v w2 ee ei er cs2 cs he hi hr b den, 1/cs2, 1/b
+    double FB[6][AFP];     // face flux cotangent
+    double G[6][AFP];      // g_c
+    double LAMB[6][AFP];   // lambda-bar_c
+    double LS[6][6][AFP];  // L row c
+    double LB[6][6][AFP];  // L-bar row c
+    double WB[6][6][AFP];  // w-bar [c][k]
+    double FK[6][6][AFP];  // f-bar [c][k]
     int act[FLUX_FACES];
 };
+static_assert(14 * FLUX_NPT + FLUX_NPT / 8 + 1 <= 36 * AFP, "step-1 staging fits in LS");
 
 template <int DIR>
 __device__ __forceinline__ void adj_face_index(const Tile& t, int f, int& i, int& j, int& p0, int& ps) {
@@ -839,7 +844,7 @@ __constant__ unsigned short kAdjVItems[90] = {
 struct AdjGhostWarp {
     double L[36], R[36], lam[6];             // L[6c + j]; R column c at R[6c + i]
     double U6[6][56];                        // rotated stencil states
-    double D[6][56], ACC[6][56], STD[6][56]; // STD becomes D-bar in place
+    double D[6][56], ACC[6][56], STD[6][56]; // STD: D-bar
     double alpha[6][5], beta[6][5], V[6][5][5];
     double v[5][6], x[5][6], ub[5][6], xb[5][6], vinf[6], vinfb[6];
     double Lb[6][6], Rb[6][6];
@@ -920,7 +925,8 @@ __device__ void ghost_vjp_warp(const Inst& I, const GhostRec& Rg, const double* 
     const double* lam = G.lam;
     const int32_t* st = reinterpret_cast<const int32_t*>(rec + GH_ST);
     const double* S = rec + GH_S;   // transposed per order: S_r[a][b] = S[off + b m + a]
-    // ---- forward: D, ACC = S d, STD = S^T d, beta, alpha, V, v
+    // ---- forward: D, ACC = S d, beta, alpha, V, v. S_r = P^T M_r P is
+    // symmetric (bc1.rs:169-175), so d beta / d d = 2 S d: S^T d is not formed
     for (int a = lane; a < 55; a += 32) {
         double s[6];
         load6(X, plane, st[a], s);
@@ -936,18 +942,15 @@ __device__ void ghost_vjp_warp(const Inst& I, const GhostRec& Rg, const double* 
     for (int a = lane; a < 55; a += 32) {
         const int r = aorder(a), m = (r + 1) * (r + 1), off = kAStOff[r], ar = a - off;
         const double* Sr = S + kASOff[r];
-        double acc[6] = {0, 0, 0, 0, 0, 0}, acct[6] = {0, 0, 0, 0, 0, 0};
+        double acc[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll 5
         for (int b = 0; b < m; ++b) {
-            const double sab = Sr[b * m + ar], sba = Sr[ar * m + b]; // S[a][b], S[b][a]
+            const double sab = Sr[b * m + ar]; // S[a][b]
 #pragma unroll
-            for (int c = 0; c < 6; ++c) {
-                const double d = G.D[c][off + b];
-                acc[c] += sab * d;  // (S d)_a
-                acct[c] += sba * d; // (S^T d)_a
-            }
+            for (int c = 0; c < 6; ++c) acc[c] += sab * G.D[c][off + b]; // (S d)_a
         }
 #pragma unroll
-        for (int c = 0; c < 6; ++c) { G.ACC[c][a] = acc[c]; G.STD[c][a] = acct[c]; }
+        for (int c = 0; c < 6; ++c) G.ACC[c][a] = acc[c];
     }
     __syncwarp();
     if (lane < 30) {
@@ -1069,7 +1072,7 @@ __device__ void ghost_vjp_warp(const Inst& I, const GhostRec& Rg, const double* 
     for (int a = lane; a < 55; a += 32) {
         const int r = aorder(a), m = (r + 1) * (r + 1), off = kAStOff[r], ar = a - off;
         for (int c = 0; c < 6; ++c) {
-            double acc = G.beta[c][r] * (G.ACC[c][a] + G.STD[c][a]);
+            double acc = G.beta[c][r] * (2.0 * G.ACC[c][a]);
             for (int k = 0; k <= r; ++k) acc += G.V[c][r][k] * rec[GH_W + kAWOff[r] + k * m + ar];
             G.STD[c][a] = acc; // D-bar
         }

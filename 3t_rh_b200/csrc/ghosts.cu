@@ -15,7 +15,8 @@
 // lambda; 10.5 KB) arrives in shared memory by one bulk copy (cp.async.bulk,
 // completion on an mbarrier) issued one ghost ahead, so the table stream
 // overlaps the arithmetic. Per ghost:
-//   1. every lane gathers its E_r stencil nodes (E_0..E_4, 55 nodes);
+//   1. every lane gathers its E_r stencil nodes (E_0..E_4, 55 nodes), one
+//      ghost ahead (the loads of the next ghost are in flight meanwhile);
 //   2. lanes spread over the 55 stencil nodes: rotate the momentum and
 //      project on the six characteristic fields (bc1.rs:209-219);
 //   3. lanes spread over the 55 rows of S_0..S_4: (S_r d_c)_a for all six c,
@@ -473,6 +474,13 @@ __global__ void __launch_bounds__(GH_WARPS * 32) k_ghosts(const Inst* __restrict
             bulk_load(G.rec[0], hrec + (size_t)heavy[g].heavy * GH_REC, GH_REC * 8, &G.bar[0]);
         }
         __syncwarp();
+        // stencil states of the warp's first ghost; later ones are gathered one
+        // ghost ahead, while the current one is processed
+        double s0[6], s1[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        {
+            const GhostRec& R0 = heavy[g];
+            gather_stencil(insts[R0.inst], hrec + (size_t)R0.heavy * GH_REC, lane, stage, s0, s1);
+        }
         for (int it = 0; g < nh; ++it, g += stride) {
             const int b = it & 1;
             const int gn = g + stride;
@@ -481,8 +489,11 @@ __global__ void __launch_bounds__(GH_WARPS * 32) k_ghosts(const Inst* __restrict
             const GhostRec Rg = heavy[g];
             const Inst& I = insts[Rg.inst];
             const bool skip = has_error(I);
-            double s0[6], s1[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-            if (!skip) gather_stencil(I, hrec + (size_t)Rg.heavy * GH_REC, lane, stage, s0, s1);
+            double n0[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, n1[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+            if (gn < nh) {
+                const GhostRec& Rn = heavy[gn];
+                gather_stencil(insts[Rn.inst], hrec + (size_t)Rn.heavy * GH_REC, lane, stage, n0, n1);
+            }
             const bool ok = __all_sync(0xffffffffu, mbar_wait(&G.bar[b], (uint32_t)((it >> 1) & 1)));
             if (!ok) {
                 if (lane == 0) report(I, 1 + 2 * stage, GH_TIMEOUT_CODE, (unsigned)Rg.gid);
@@ -491,6 +502,8 @@ __global__ void __launch_bounds__(GH_WARPS * 32) k_ghosts(const Inst* __restrict
             }
             if (!skip) heavy_ghost(I, Rg, G, G.rec[b], lane, stage, row1, row2, vitem, s0, s1);
             __syncwarp();
+#pragma unroll
+            for (int q = 0; q < 6; ++q) { s0[q] = n0[q]; s1[q] = n1[q]; }
         }
     }
 }

@@ -48,6 +48,19 @@ def heavy_ghost_flops(kind="far_field"):
     return rotate_derived_lr + data + beta + vk + weights + post + taylor
 
 
+# Algorithmic HBM bytes of one heavy ghost per stage: its GhostBC tables
+# (bc1.rs:50-57: S_0..S_4 979, w 225, d 5 doubles; the E_r stencil as 55
+# 4-byte node indices), which no cache holds across stages at scale, plus the
+# ghost value written (6 doubles). The stencil states are shared with the
+# neighbouring ghosts and cells and are not counted.
+HEAVY_GHOST_BYTES = (979 + 225 + 5) * 8 + 55 * 4 + 6 * 8
+
+
+def ghost_launch_bytes(n_heavy):
+    """Algorithmic bytes of one stage's ghost update (heavy ghosts' tables)."""
+    return n_heavy * HEAVY_GHOST_BYTES
+
+
 def step_flops(n_fluid, n_xfaces, n_yfaces, n_ghosts, n_heavy, diffusion=False, source=False):
     """Algorithmic FLOPs of one RK3 step (3 stages + the dt reduction)."""
     per_stage = (n_xfaces + n_yfaces) * (FACE_FLUX + (DIFFUSION if diffusion else 0))

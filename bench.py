@@ -41,6 +41,8 @@ WORKLOADS = {
     "planar": dict(kind="planar", name="Mach-2 planar shock, 1024x8, y-periodic, diffusion+exchange on"),
     "batch256": dict(kind="batch", n=256, name="256 half-cylinder instances, nx in {61,91,121}, ny = 4(nx-1)+1, "
                      "Mach U[2,4], omega_ei/omega_er log-U[0.1,10] x 1.0, seed 20261203"),
+    # the first 24 instances of batch256: the small case of the ncu captures
+    "batch24": dict(kind="batch", n=24, name="the first 24 of the batch256 instances (profiling case)"),
 }
 PLANAR_PARAMS = dict(kappa_e=1e-3, kappa_i=1e-3, kappa_r=1e-3, omega_ei=1.0, omega_er=1.0, periodic_ly=0.03125)
 CFL = 0.05
@@ -48,6 +50,20 @@ CFL = 0.05
 # launch, from an ncu capture of `bench.py --steps 3 --warmup 3 --no-cpu
 # --no-e2e` (FMA build); None where no capture exists
 FLUX_TRAFFIC_BYTES = {"cyl961": 651.5e6}
+# DRAM bytes per heavy ghost of one stage's ghost update (k_ghost_prep +
+# k_ghosts), from an ncu capture on 24 batch instances (84,000 heavy ghosts),
+# scaled by the heavy-ghost count; None until captured
+GHOST_TRAFFIC_PER_HEAVY = None
+FALLBACK_HBM_GBS = 6650.0
+
+
+def hbm_peak():
+    """Measured copy bandwidth of this pool's B200s (GB/s) and its source."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (of measured)"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback 6.65 TB/s (of fallback)"
 
 
 def make_field(rh, wl):
@@ -318,16 +334,39 @@ def run_batch(args, rh, flops, torch, dist, world, rank, local):
     value, ms = replica_value(ms, cells, args.steps, dist, f"cuda:{local}")
     sampler.stop()
     clocks = sampler.summary()
-    prof = b.profile_steps(min(args.steps, 10), CFL)
+    k_prof = min(args.steps, 10)
+    prof = b.profile_steps(k_prof, CFL)
     flux_ms, flux_n = prof["flux"]
     achieved = fl_launch / (flux_ms / flux_n * 1e-3) / 1e12
     peak = rh.api.fp64_peak_tflops(local)
     total_prof_ms = sum(v[0] for v in prof.values())
+    share = {k: v[0] / total_prof_ms for k, v in prof.items()}
+    n_heavy = int(sum(g.n_heavy() for g in grids))
+    ghost_stage_ms = prof["ghosts"][0] / (3 * k_prof)
+    g_bytes = flops.ghost_launch_bytes(n_heavy)
+    hbm, hbm_src = hbm_peak()
+    g_achieved = g_bytes / (ghost_stage_ms * 1e-3) / 1e9
+    rl_flux = {"bound": "fp64", "kernel": "k_flux (x+y interface WENO5 fluxes, all instances)",
+               "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+               "traffic": FLUX_TRAFFIC_BYTES.get(args.workload) if not args.exact else None,
+               "traffic_unit": "bytes per launch", "peak_source": "measured DFMA loop on this GPU (rh3t_fp64_peak)",
+               "flops_per_launch": fl_launch, "launch_ms": flux_ms / flux_n}
+    rl_ghost = {"bound": "hbm", "kernel": "k_ghost_prep + k_ghosts (one stage's ghost update, all instances)",
+                "achieved": g_achieved, "peak": hbm, "unit": "GB/s", "frac": g_achieved / hbm,
+                "traffic": None if GHOST_TRAFFIC_PER_HEAVY is None or args.exact
+                else GHOST_TRAFFIC_PER_HEAVY * n_heavy,
+                "traffic_unit": "bytes per stage", "peak_source": hbm_src,
+                "bytes_per_launch": g_bytes, "launch_ms": ghost_stage_ms,
+                "bytes_model": f"{flops.HEAVY_GHOST_BYTES} B of GhostBC tables per heavy ghost x {n_heavy}"}
+    dominant = "ghosts" if share["ghosts"] >= share["flux"] else "flux"
+    roofline = dict(rl_ghost if dominant == "ghosts" else rl_flux)
+    roofline.update({"kernel_share": share, "step_tflops": step_fl / (ms / args.steps * 1e-3) / 1e12,
+                     "step_flops": step_fl, "other": {"flux": rl_flux} if dominant == "ghosts" else {"ghosts": rl_ghost}})
 
     # the plain GPU path on the same instances, one instance at a time
     k_plain = max(5, min(args.steps, 20))
     plain_ms, plain_cells = 0.0, 0
-    for f, g in zip(fields, grids):
+    for f, g in (zip(fields, grids) if not args.no_plain else ()):
         sv = rh.Solver(f, g, device=local, exact=args.exact)
         sv.advance(3, CFL)
         st = torch.cuda.ExternalStream(sv.stream, device=torch.device(f"cuda:{local}"))
@@ -340,7 +379,7 @@ def run_batch(args, rh, flops, torch, dist, world, rank, local):
         plain_ms += e0.elapsed_time(e1)
         plain_cells += int(f.fluid.sum())
         sv.close()
-    plain_value = plain_cells * k_plain / (plain_ms * 1e-3)
+    plain_value = plain_cells * k_plain / (plain_ms * 1e-3) if plain_ms > 0 else None
 
     e2e = None
     if not args.no_e2e:
@@ -364,7 +403,8 @@ def run_batch(args, rh, flops, torch, dist, world, rank, local):
 
     adj = None
     if not args.no_adjoint:
-        adj = adjoint_bench(rh, torch, local, args.exact)
+        adj = adjoint_bench(rh, torch, local, args.exact, nsteps=args.adjoint_steps,
+                            ckpt=min(20, args.adjoint_steps), n=args.adjoint_instances)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -391,17 +431,11 @@ def run_batch(args, rh, flops, torch, dist, world, rank, local):
                        "field_setup_s": round(fields_s, 3),
                        "tile_shapes": {f"{e['nx']}x{e['ny']}": e["shape"] for e in tune}},
             "instances_per_s": value / cells * b.n,
-            "plain_one_at_a_time": {"value": plain_value, "unit": "cell-updates/s", "steps_per_instance": k_plain,
-                                    "batched_speedup": value / plain_value},
+            "plain_one_at_a_time": None if plain_value is None else {
+                "value": plain_value, "unit": "cell-updates/s", "steps_per_instance": k_plain,
+                "batched_speedup": value / plain_value},
             "adjoint": adj,
-            "roofline": {"bound": "fp64", "kernel": "k_flux (x+y interface WENO5 fluxes, all instances)",
-                         "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                         "traffic": FLUX_TRAFFIC_BYTES.get(args.workload) if not args.exact else None,
-                         "traffic_unit": "bytes per launch",
-                         "peak_source": "measured DFMA loop on this GPU (rh3t_fp64_peak)",
-                         "flops_per_launch": fl_launch, "launch_ms": flux_ms / flux_n,
-                         "kernel_share": {k: v[0] / total_prof_ms for k, v in prof.items()},
-                         "step_tflops": step_fl / (ms / args.steps * 1e-3) / 1e12, "step_flops": step_fl},
+            "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": launches,
@@ -422,6 +456,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the one-instance-at-a-time comparison")
+    ap.add_argument("--adjoint-steps", type=int, default=200)
+    ap.add_argument("--adjoint-instances", type=int, default=32)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
