@@ -51,9 +51,11 @@ CFL = 0.05
 # --no-e2e` (FMA build); None where no capture exists
 FLUX_TRAFFIC_BYTES = {"cyl961": 651.5e6}
 # DRAM bytes per heavy ghost of one stage's ghost update (k_ghost_prep +
-# k_ghosts), from an ncu capture on 24 batch instances (84,000 heavy ghosts),
-# scaled by the heavy-ghost count; None until captured
-GHOST_TRAFFIC_PER_HEAVY = None
+# k_ghosts) and per active face of one k_flux launch, from ncu captures on
+# the batch24 workload (84,000 heavy ghosts, 1,714,456 faces), scaled by the
+# heavy-ghost and face counts of the batched workloads
+GHOST_TRAFFIC_PER_HEAVY = (902.84e6 + 7.47e6 + 15.32e6 + 9.71e6) / 84000
+FLUX_TRAFFIC_PER_FACE = (77.82e6 + 42.39e6) / 1714456
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -310,9 +312,10 @@ def run_batch(args, rh, flops, torch, dist, world, rank, local):
     b = rh.Batch(fields, grids, device=local, exact=args.exact)
     cells = int(sum(int(f.fluid.sum()) for f in fields))
     tune = b.autotune(reps=5)
-    step_fl, fl_launch = 0.0, 0.0
+    step_fl, fl_launch, n_faces = 0.0, 0.0, 0
     for f, g in zip(fields, grids):
         nxf, nyf = flops.face_counts(f.fluid, f.grid.nx, f.grid.ny)
+        n_faces += nxf + nyf
         step_fl += flops.step_flops(int(f.fluid.sum()), nxf, nyf, g.len(), g.n_heavy(), False, True)
         fl_launch += flops.flux_launch_flops(nxf, nyf, False)
     stream = torch.cuda.ExternalStream(b.stream, device=torch.device(f"cuda:{local}"))
@@ -348,7 +351,7 @@ def run_batch(args, rh, flops, torch, dist, world, rank, local):
     g_achieved = g_bytes / (ghost_stage_ms * 1e-3) / 1e9
     rl_flux = {"bound": "fp64", "kernel": "k_flux (x+y interface WENO5 fluxes, all instances)",
                "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-               "traffic": FLUX_TRAFFIC_BYTES.get(args.workload) if not args.exact else None,
+               "traffic": None if args.exact else FLUX_TRAFFIC_PER_FACE * n_faces,
                "traffic_unit": "bytes per launch", "peak_source": "measured DFMA loop on this GPU (rh3t_fp64_peak)",
                "flops_per_launch": fl_launch, "launch_ms": flux_ms / flux_n}
     rl_ghost = {"bound": "hbm", "kernel": "k_ghost_prep + k_ghosts (one stage's ghost update, all instances)",
