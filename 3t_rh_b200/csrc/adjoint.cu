@@ -850,6 +850,7 @@ struct AdjGhostWarp {
     double Lb[6][6], Rb[6][6];
     double vb[5][6];
     double Z[6][6];
+    double omm[6][5]; // omega_r * omega-bar_r per field
 };
 
 __device__ __forceinline__ int aorder(int a) { return a < 1 ? 0 : (a < 5 ? 1 : (a < 14 ? 2 : (a < 30 ? 3 : 4))); }
@@ -905,6 +906,12 @@ __global__ void __launch_bounds__(AG_LR_THREADS) k_adj_ghost_lr(const Inst* __re
     }
 }
 
+// L2 prefetch of a ghost's record by the bulk-copy engine (16-byte aligned,
+// size a multiple of 16; nothing waits on it)
+__device__ __forceinline__ void prefetch_record_l2(const double* rec) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(rec), "r"((unsigned)(GH_REC * 8)) : "memory");
+}
+
 // one heavy (FarField) ghost per warp; gb from W at the ghost node
 __device__ void ghost_vjp_warp(const Inst& I, const GhostRec& Rg, const double* __restrict__ rec,
                                const double* __restrict__ X, const double* __restrict__ W, double* __restrict__ Ub,
@@ -912,6 +919,8 @@ __device__ void ghost_vjp_warp(const Inst& I, const GhostRec& Rg, const double* 
     const DevParams& P = I.P;
     const long long plane = I.plane;
     const double nx = Rg.nx, ny = Rg.ny;
+    // the record's S_r and w are read in steps below: have them in L2 first
+    if (lane == 0) prefetch_record_l2(rec);
     // L, R, lambda at the nearest node of X (k_adj_ghost_lr)
     for (int e = lane; e < 78; e += 32) {
         const double v = slot[e];
@@ -1048,24 +1057,24 @@ __device__ void ghost_vjp_warp(const Inst& I, const GhostRec& Rg, const double* 
         const double bu[6] = {b[0], b[1] * nx - b[2] * ny, b[1] * ny + b[2] * nx, b[3], b[4], b[5]};
         for (int c = 0; c < 6; ++c) atomicAdd(&pbar_k[c], bu[c]);
     }
-    // v[k][c] = sum_r (alpha_r / sum) V_r^k -> V-bar, alpha-bar -> beta-bar
-    if (lane < 6) {
-        const int c = lane;
-        double asum = 0.0;
-        for (int r = 0; r < 5; ++r) asum += G.alpha[c][r];
-        double om[5], omb[5], m = 0.0;
-        for (int r = 0; r < 5; ++r) {
-            om[r] = G.alpha[c][r] / asum;
-            omb[r] = 0.0;
-            for (int k = 0; k < 5; ++k) omb[r] += G.V[c][r][k] * G.vb[k][c];
-            m += om[r] * omb[r];
-        }
-        for (int r = 0; r < 5; ++r) {
-            const double ab = (omb[r] - m) / asum;
-            // alpha = d (eps + beta)^-q
-            G.beta[c][r] = -P.weno_q * ab * G.alpha[c][r] / (P.eps + G.beta[c][r]); // now beta-bar
-            for (int k = 0; k < 5; ++k) G.V[c][r][k] = om[r] * G.vb[k][c];          // now V-bar
-        }
+    // v[k][c] = sum_r (alpha_r / sum) V_r^k -> V-bar, alpha-bar -> beta-bar,
+    // lanes (c, r)
+    const int oc = lane / 5, orr = lane - 5 * (lane / 5);
+    double asum = 0.0, om = 0.0, omb = 0.0;
+    if (lane < 30) {
+        for (int r = 0; r < 5; ++r) asum += G.alpha[oc][r];
+        om = G.alpha[oc][orr] / asum;
+        for (int k = 0; k < 5; ++k) omb += G.V[oc][orr][k] * G.vb[k][oc];
+        G.omm[oc][orr] = om * omb;
+    }
+    __syncwarp();
+    if (lane < 30) {
+        double m = 0.0;
+        for (int r = 0; r < 5; ++r) m += G.omm[oc][r];
+        const double ab = (omb - m) / asum;
+        // alpha = d (eps + beta)^-q
+        G.beta[oc][orr] = -P.weno_q * ab * G.alpha[oc][orr] / (P.eps + G.beta[oc][orr]); // now beta-bar
+        for (int k = 0; k < 5; ++k) G.V[oc][orr][k] = om * G.vb[k][oc];                 // now V-bar
     }
     __syncwarp();
     // D-bar over the 55 nodes: beta = d^T S d, V = w . d
