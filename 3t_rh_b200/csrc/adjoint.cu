@@ -278,6 +278,58 @@ __device__ __forceinline__ void r_base_vjp(const double base[5], const DevParams
     bb[4] += be[2] + GR * gr * hc * bcs;
 }
 
+// r_base_vjp for the two columns c0, c0 + 1 of R-bar (the other columns
+// zero): the part of the Roe base cotangent they carry, added to bb
+template <int DIR>
+__device__ __forceinline__ void r_base_vjp2(const double base[5], const DevParams& P, int c0, const double Rb2[2][6],
+                                            const double lamb2[2], double bb[5]) {
+    const double GE = P.gamma_e, GI = P.gamma_i, GR = P.gamma_r;
+    const double gi = GI - 1.0, ge = GE - 1.0, gr = GR - 1.0;
+    const double gt = gi + ge + gr;
+    const double u = base[0], v = base[1];
+    const double cs = sqrt(GE * ge * base[2] + GI * gi * base[3] + GR * gr * base[4]);
+    const double vel = DIR == 0 ? u : v;
+    double bvel = 0.0, bcs = 0.0, bw2 = 0.0, bu = 0.0, bv = 0.0, be[3] = {0.0, 0.0, 0.0};
+    const double Gk[3] = {GE, GI, GR}, gk[3] = {ge, gi, gr};
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int c = c0 + h;
+        const double* r = Rb2[h];
+        if (c == 0 || c == 5) { // acoustic: (1, [vel -+ cs], ..., G_k e_k + w2/6 -+ vel cs/3)
+            const double sg = c == 0 ? -1.0 : 1.0;
+            if (DIR == 0) { bu += r[1]; bcs += sg * r[1]; bv += r[2]; }
+            else { bu += r[1]; bv += r[2]; bcs += sg * r[2]; }
+            for (int k = 0; k < 3; ++k) {
+                be[k] += Gk[k] * r[3 + k];
+                bw2 += r[3 + k] * K6;
+                bvel += sg * cs * K3 * r[3 + k];
+                bcs += sg * vel * K3 * r[3 + k];
+            }
+            bcs += sg * lamb2[h];
+        } else if (c == (DIR == 0 ? 4 : 1)) { // transverse: unit momentum, (t/3, t/3, t/3)
+            const double t3 = (r[3] + r[4] + r[5]) * K3;
+            if (DIR == 0) bv += t3;
+            else bu += t3;
+        } else { // species k: (1, u, v, ..., gt w2 / (6 g_k) at row 3 + k)
+            const int k = DIR == 0 ? c - 1 : c - 2;
+            bu += r[1];
+            bv += r[2];
+            bw2 += gt * K6 / gk[k] * r[3 + k];
+        }
+        bvel += lamb2[h];
+    }
+    if (DIR == 0) bu += bvel;
+    else bv += bvel;
+    bu += 2.0 * u * bw2;
+    bv += 2.0 * v * bw2;
+    const double hc = 0.5 / cs;
+    bb[0] += bu;
+    bb[1] += bv;
+    bb[2] += be[0] + GE * ge * hc * bcs;
+    bb[3] += be[1] + GI * gi * hc * bcs;
+    bb[4] += be[2] + GR * gr * hc * bcs;
+}
+
 // L = R^-1, so dL = -L dR L and the cotangent Lb of L is one of R:
 // Rb -= L^T Lb L^T. Rb[c][i] = dJ/dR[i][c], Lb[c][j] = dJ/dL[c][j],
 // L[c][j] = L[6c + j].
@@ -477,47 +529,64 @@ __device__ void adj_flux_tile(const Inst& I, const Tile& t, const double* __rest
         const bool on = f < FLUX_FACES && S.act[f];
         double bb[5] = {0, 0, 0, 0, 0};
         if (on) {
-            double Rb[6][6], lamb[6];
-            for (int c2 = 0; c2 < 6; ++c2) {
-                const bool mine = (c2 >> 1) == part;
-                lamb[c2] = mine ? S.LAMB[c2][f] : 0.0;
-                for (int m = 0; m < 6; ++m) Rb[c2][m] = mine ? S.FB[m][f] * S.G[c2][f] : 0.0;
+            // own columns c0, c0 + 1 of R-bar: Fb g_c^T, then -= sum_j L[j][i] Z[j][c]
+            // with Z[j][c] = sum_k Lb[j][k] L[c][k]
+            const int c0 = 2 * part;
+            double Rb2[2][6], lamb2[2], Z0[6] = {}, Z1[6] = {};
+            lamb2[0] = S.LAMB[c0][f];
+            lamb2[1] = S.LAMB[c0 + 1][f];
+            const double g0 = S.G[c0][f], g1 = S.G[c0 + 1][f];
+#pragma unroll
+            for (int m = 0; m < 6; ++m) {
+                const double fb = S.FB[m][f];
+                Rb2[0][m] = fb * g0;
+                Rb2[1][m] = fb * g1;
             }
-            // Rb[c][i] -= sum_j L[j][i] Z[j][c], Z[j][c] = sum_k Lb[j][k] L[c][k], own columns c
-            for (int c2 = 2 * part; c2 < 2 * part + 2; ++c2) {
-                double Z[6];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+                const double l0 = S.LS[c0][k][f], l1 = S.LS[c0 + 1][k][f];
+#pragma unroll
                 for (int j = 0; j < 6; ++j) {
-                    double acc = 0.0;
-                    for (int k = 0; k < 6; ++k) acc += S.LB[j][k][f] * S.LS[c2][k][f];
-                    Z[j] = acc;
+                    const double lb = S.LB[j][k][f];
+                    Z0[j] += lb * l0;
+                    Z1[j] += lb * l1;
                 }
-                for (int i = 0; i < 6; ++i) {
-                    double acc = 0.0;
-                    for (int j = 0; j < 6; ++j) acc += S.LS[j][i][f] * Z[j];
-                    Rb[c2][i] -= acc;
+            }
+#pragma unroll
+            for (int i = 0; i < 6; ++i) {
+                double a0 = 0.0, a1 = 0.0;
+#pragma unroll
+                for (int j = 0; j < 6; ++j) {
+                    const double l = S.LS[j][i][f];
+                    a0 += l * Z0[j];
+                    a1 += l * Z1[j];
                 }
+                Rb2[0][i] -= a0;
+                Rb2[1][i] -= a1;
             }
             const Roe q = adj_load_q(S, f);
             const double base[5] = {q.u, q.v, q.ee, q.ei, q.er};
-            r_base_vjp<DIR>(base, P, Rb, lamb, bb);
+            r_base_vjp2<DIR>(base, P, c0, Rb2, lamb2, bb);
         }
         // per face and point k of this part: V_k = sum_c wbar_ck L_c and
         // VF_k = sum_c fbar_ck L_c (the point sums of 3b read these)
-        double V[2][6], VF[2][6];
-        if (on)
-            for (int h = 0; h < 2; ++h) {
-                const int k = 2 * part + h;
+        double V[2][6] = {}, VF[2][6] = {};
+        if (on) {
+            const int k0 = 2 * part;
+#pragma unroll
+            for (int c2 = 0; c2 < 6; ++c2) {
+                const double w0 = S.WB[c2][k0][f], w1 = S.WB[c2][k0 + 1][f];
+                const double q0 = S.FK[c2][k0][f], q1 = S.FK[c2][k0 + 1][f];
+#pragma unroll
                 for (int m = 0; m < 6; ++m) {
-                    double a = 0.0, b = 0.0;
-                    for (int c2 = 0; c2 < 6; ++c2) {
-                        const double l = S.LS[c2][m][f];
-                        a += S.WB[c2][k][f] * l;
-                        b += S.FK[c2][k][f] * l;
-                    }
-                    V[h][m] = a;
-                    VF[h][m] = b;
+                    const double l = S.LS[c2][m][f];
+                    V[0][m] += w0 * l;
+                    V[1][m] += w1 * l;
+                    VF[0][m] += q0 * l;
+                    VF[1][m] += q1 * l;
                 }
             }
+        }
         __syncthreads(); // LB, WB, FK, G and LAMB are read: reuse them
         if (on) {
             if (part == 0) for (int m = 0; m < 5; ++m) S.FK[0][m][f] = bb[m];
