@@ -11,6 +11,7 @@ reference's message.
 """
 import ctypes as C
 import math
+import os
 
 import numpy as np
 
@@ -376,7 +377,43 @@ class GhostGrid:
 
 
 # ------------------------------------------------------------------ device solver
-class Solver:
+class _SnapshotIO:
+    """RH3TBIN1 snapshots, restart and the energy-split diagnostic of one
+    instance (io.rs save_data / load_data, py_utils/energy_split.py)."""
+
+    def snapshot(self, path, k=0):
+        """Write instance k's state to `path` (RH3TBIN1); returns before the
+        file is written (snapshot_wait joins)."""
+        self._check(self.L.rh3t_snapshot(self.h, int(k), os.fsencode(path)))
+
+    def snapshot_wait(self):
+        self._check(self.L.rh3t_snapshot_wait(self.h))
+
+    def save_data(self, filename, k=0, directory="data_new"):
+        """io.rs:25-99 save_data: `directory`/`filename`, written through a
+        .tmp file and a rename; waits for the file."""
+        os.makedirs(directory, exist_ok=True)
+        self.snapshot(os.path.join(directory, filename), k)
+        self.snapshot_wait()
+
+    def load_data(self, path, k=0):
+        """io.rs:101-123 load_data: instance k's state and time from `path`."""
+        self._check(self.L.rh3t_restart(self.h, int(k), os.fsencode(path)))
+
+    def energy_split(self, k=0):
+        """py_utils/energy_split.py for instance k: max, mean and rms of
+        |Ee-Ei|, |Ee-Er|, |Ei-Er| over fluid nodes, and (x, y) of the max
+        |Ee-Er| (first in j-major order)."""
+        out = np.zeros(12)
+        self._check(self.L.rh3t_energy_split(self.h, int(k), out.ctypes.data))
+        names = ("max_Ee_Ei", "max_Ee_Er", "max_Ei_Er", "mean_Ee_Ei", "mean_Ee_Er", "mean_Ei_Er", "rms_Ee_Ei",
+                 "rms_Ee_Er", "rms_Ei_Er", "x_max_Ee_Er", "y_max_Ee_Er")
+        d = dict(zip(names, out[:11].tolist()))
+        d["n_fluid"] = int(out[11])
+        return d
+
+
+class Solver(_SnapshotIO):
     """Device copy of a Field + GhostGrid + the l() scratch (main.rs:45-67):
     one rh3t_ctx on one CUDA stream."""
 
@@ -473,7 +510,7 @@ class Solver:
         return self.L.rh3t_stream(self.h)
 
 
-class Batch:
+class Batch(_SnapshotIO):
     """Independent instances (Field + GhostGrid each, any sizes, parameters
     and BCs) resident together on one GPU (rh3t_batch_create). Every kernel
     launch covers all instances; each instance has its own dt reduction, time
@@ -531,10 +568,15 @@ class Batch:
         t = _arr(times, np.float64)
         self._check(self.L.rh3t_upload_batch(self.h, v.ctypes.data, t.ctypes.data))
 
-    def download_values(self):
-        """(total_cells x 6 values of all instances, times[n])"""
-        out = np.zeros((int(self.offsets[-1]), 6))
-        t = np.zeros(self.n)
+    def download_values(self, out=None, times=None):
+        """(total_cells x 6 values of all instances, times[n]); out / times
+        (float64, C-contiguous, e.g. pinned host memory) receive the copy
+        when given."""
+        if out is None:
+            out = np.zeros((int(self.offsets[-1]), 6))
+        elif out.dtype != np.float64 or not out.flags.c_contiguous or out.size != int(self.offsets[-1]) * 6:
+            raise ValueError("out must be a C-contiguous float64 array of total_cells x 6")
+        t = np.zeros(self.n) if times is None else times
         self._check(self.L.rh3t_download_batch(self.h, out.ctypes.data, t.ctypes.data))
         return out, t
 

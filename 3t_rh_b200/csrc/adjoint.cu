@@ -948,7 +948,7 @@ __global__ void __launch_bounds__(AG_LR_THREADS) k_adj_ghost_lr(const Inst* __re
     if (g < nh) {
         const GhostRec Rg = heavy[g];
         const Inst& I = insts[Rg.inst];
-        if (!has_error(I) && Rg.kind == BC_FAR_FIELD) {
+        if (!has_error(I)) {
             double q6[6];
             const Roe q = nearest_roe(I, Rg, Xb + I.aoff, q6);
             double* o = lr_smem + threadIdx.x;
@@ -973,6 +973,160 @@ __global__ void __launch_bounds__(AG_LR_THREADS) k_adj_ghost_lr(const Inst* __re
         double* o = slots + (size_t)gj * AG_SLOT;
         for (int e = lane; e < 78; e += 32) o[e] = lr_smem[e * ST + t];
     }
+}
+
+// A x = b for a 6x6 system by LU with partial pivoting (the forward's
+// bc1.rs:467-469 solve6); A is overwritten; false if singular
+__device__ bool lu_solve6(double A[6][6], double b[6]) {
+    int piv[6];
+    for (int j = 0; j < 6; ++j) {
+        int p = j;
+        double mx = fabs(A[j][j]);
+        for (int i = j + 1; i < 6; ++i)
+            if (fabs(A[i][j]) > mx) { mx = fabs(A[i][j]); p = i; }
+        piv[j] = p;
+        if (A[p][j] == 0.0) return false;
+        if (p != j)
+            for (int k = 0; k < 6; ++k) { const double t = A[j][k]; A[j][k] = A[p][k]; A[p][k] = t; }
+        const double rcp = 1.0 / A[j][j];
+        for (int i = j + 1; i < 6; ++i) A[i][j] *= rcp;
+        for (int k = j + 1; k < 6; ++k)
+            for (int i = j + 1; i < 6; ++i) A[i][k] -= A[i][j] * A[j][k];
+    }
+    for (int j = 0; j < 6; ++j)
+        if (piv[j] != j) { const double t = b[j]; b[j] = b[piv[j]]; b[piv[j]] = t; }
+    for (int k = 0; k < 6; ++k)
+        for (int i = k + 1; i < 6; ++i) b[i] -= b[k] * A[i][k];
+    for (int k = 5; k >= 0; --k) {
+        b[k] /= A[k][k];
+        for (int i = 0; i < k; ++i) b[i] -= b[k] * A[i][k];
+    }
+    return true;
+}
+
+// Wall (ILW, bc1.rs:691-756) or Outflow (LODI, bc1.rs:760-828) rows in
+// reverse, on one lane: from ub[k] (cotangents of u_k) and the forward's v,
+// L, R to vb[k] (cotangents of v_k), Rb (R columns) and Lb (L rows, from the
+// ILW systems). Wall: u_0 = A_0^-1 r_0 with A_0 = L but row 0 = e_1 and
+// r_0 = v_0 but r_0[0] = 0, u_1 = A_1^-1 r_1 with row 0 of A_1 the ILW
+// momentum row of u_0, u_k = R v_k (k >= 2); so r-bar = A^-T u-bar and
+// A-bar = -r-bar u^T. Outflow: u_k = R r_k with r_k = v_k except
+// r_1[0] = l_1(u_0) / lambda_1(u_0) when lambda_1 = u_n - a < 0 (its
+// gradient by dual numbers). Returns false if an ILW system is singular.
+__device__ __noinline__ bool wall_outflow_vjp(const Inst& I, const GhostRec& Rg, AdjGhostWarp& G) {
+    const DevParams& P = I.P;
+    const double* L = G.L; // L[c][j] = L[6c + j]
+    const double* Rc = G.R; // R[i][c] = Rc[6c + i]
+    double Rb[6][6], Lb[6][6], vb[5][6];
+    for (int c = 0; c < 6; ++c)
+        for (int i = 0; i < 6; ++i) { Rb[c][i] = 0.0; Lb[c][i] = 0.0; }
+    for (int k = 0; k < 5; ++k)
+        for (int c = 0; c < 6; ++c) vb[k][c] = 0.0;
+    // u_k = R v_k, k = 2..4 (both kinds)
+    for (int k = 2; k <= 4; ++k)
+        for (int c = 0; c < 6; ++c) {
+            double acc = 0.0;
+            for (int i = 0; i < 6; ++i) {
+                acc += Rc[6 * c + i] * G.ub[k][i];
+                Rb[c][i] += G.ub[k][i] * G.v[k][c];
+            }
+            vb[k][c] = acc;
+        }
+    double u0b[6];
+    for (int c = 0; c < 6; ++c) u0b[c] = G.ub[0][c];
+    if (Rg.kind == BC_WALL) {
+        const double gi = P.gamma_i - 1.0, ge = P.gamma_e - 1.0, gr = P.gamma_r - 1.0, gt = gi + ge + gr;
+        double A0[6][6], u0[6], A1[6][6], u1[6], T[6][6];
+        for (int i = 0; i < 6; ++i)
+            for (int c = 0; c < 6; ++c) A0[i][c] = i == 0 ? (c == 1 ? 1.0 : 0.0) : L[6 * i + c];
+        for (int c = 0; c < 6; ++c) u0[c] = c == 0 ? 0.0 : G.v[0][c];
+        for (int i = 0; i < 6; ++i)
+            for (int c = 0; c < 6; ++c) T[i][c] = A0[i][c];
+        if (!lu_solve6(T, u0)) return false;
+        const double a1 = u0[0], a3 = u0[2];
+        const double row1[6] = {-gt * a3 * a3 / (6.0 * a1 * a1), 0.0, gt * a3 / (6.0 * a1), -ge, -gi, -gr};
+        for (int i = 0; i < 6; ++i)
+            for (int c = 0; c < 6; ++c) A1[i][c] = i == 0 ? row1[c] : L[6 * i + c];
+        for (int c = 0; c < 6; ++c) u1[c] = c == 0 ? 0.0 : G.v[1][c];
+        for (int i = 0; i < 6; ++i)
+            for (int c = 0; c < 6; ++c) T[i][c] = A1[i][c];
+        if (!lu_solve6(T, u1)) return false;
+        // k = 1: r1-bar = A1^-T u1-bar, A1-bar = -r1-bar u1^T
+        double r1b[6];
+        for (int c = 0; c < 6; ++c) r1b[c] = G.ub[1][c];
+        for (int i = 0; i < 6; ++i)
+            for (int c = 0; c < 6; ++c) T[i][c] = A1[c][i];
+        if (!lu_solve6(T, r1b)) return false;
+        for (int c = 1; c < 6; ++c) vb[1][c] = r1b[c];
+        for (int i = 1; i < 6; ++i)
+            for (int c = 0; c < 6; ++c) Lb[i][c] -= r1b[i] * u1[c];
+        // row 0 of A1 = the ILW row of u0 (u0[0], u0[2])
+        const double b0 = -r1b[0] * u1[0], b2 = -r1b[0] * u1[2];
+        u0b[0] += b0 * (gt * a3 * a3 / (3.0 * a1 * a1 * a1)) + b2 * (-gt * a3 / (6.0 * a1 * a1));
+        u0b[2] += b0 * (-gt * a3 / (3.0 * a1 * a1)) + b2 * (gt / (6.0 * a1));
+        // k = 0
+        for (int i = 0; i < 6; ++i)
+            for (int c = 0; c < 6; ++c) T[i][c] = A0[c][i];
+        if (!lu_solve6(T, u0b)) return false;
+        for (int c = 1; c < 6; ++c) vb[0][c] = u0b[c];
+        for (int i = 1; i < 6; ++i)
+            for (int c = 0; c < 6; ++c) Lb[i][c] -= u0b[i] * u0[c];
+    } else {
+        const DevBC& bc = I.bcs[Rg.bc];
+        // forward: u0 = R v0, the LODI row test on it
+        DualN<6> q[6];
+        for (int i = 0; i < 6; ++i) {
+            double acc = 0.0;
+            for (int c = 0; c < 6; ++c) acc += Rc[6 * c + i] * G.v[0][c];
+            q[i] = DualN<6>::var(acc, i);
+        }
+        const DualN<6> rho0 = q[0], un0 = q[1] / rho0, ut0 = q[2] / rho0;
+        const DualN<6> w2 = un0 * un0 + ut0 * ut0;
+        const DualN<6> ee1 = q[3] / rho0 - w2 * K6, ei1 = q[4] / rho0 - w2 * K6, er1 = q[5] / rho0 - w2 * K6;
+        const double ge = P.gamma_e - 1.0, gi = P.gamma_i - 1.0, gr = P.gamma_r - 1.0;
+        const DualN<6> p0 = rho0 * (ge * ee1 + gi * ei1 + gr * er1);
+        const DualN<6> a = sqrt(P.gamma_e * ge * ee1 + P.gamma_i * gi * ei1 + P.gamma_r * gr * er1);
+        const DualN<6> lambda1 = un0 - a;
+        const bool lodi = lambda1.v < 0.0;
+        double rhs1[6];
+        for (int c = 0; c < 6; ++c) rhs1[c] = G.v[1][c];
+        DualN<6> g;
+        if (lodi) {
+            const DualN<6> ml = fabs(un0 / a);
+            const DualN<6> l1 = bc.sigma * (1.0 - ml * ml) * a / bc.l_domain * (p0 - bc.p_inf);
+            g = l1 / lambda1;
+            rhs1[0] = g.v;
+        }
+        // k = 1: u1 = R rhs1
+        double r1b[6];
+        for (int c = 0; c < 6; ++c) {
+            double acc = 0.0;
+            for (int i = 0; i < 6; ++i) {
+                acc += Rc[6 * c + i] * G.ub[1][i];
+                Rb[c][i] += G.ub[1][i] * rhs1[c];
+            }
+            r1b[c] = acc;
+        }
+        for (int c = 0; c < 6; ++c) vb[1][c] = r1b[c];
+        if (lodi) {
+            vb[1][0] = 0.0;
+            for (int i = 0; i < 6; ++i) u0b[i] += r1b[0] * g.d[i];
+        }
+        // k = 0: u0 = R v0
+        for (int c = 0; c < 6; ++c) {
+            double acc = 0.0;
+            for (int i = 0; i < 6; ++i) {
+                acc += Rc[6 * c + i] * u0b[i];
+                Rb[c][i] += u0b[i] * G.v[0][c];
+            }
+            vb[0][c] = acc;
+        }
+    }
+    for (int c = 0; c < 6; ++c)
+        for (int i = 0; i < 6; ++i) { G.Rb[c][i] = Rb[c][i]; G.Lb[c][i] = Lb[c][i]; }
+    for (int k = 0; k < 5; ++k)
+        for (int c = 0; c < 6; ++c) G.vb[k][c] = vb[k][c];
+    return true;
 }
 
 // L2 prefetch of a ghost's record by the bulk-copy engine (16-byte aligned,
@@ -1090,6 +1244,14 @@ __device__ void ghost_vjp_warp(const Inst& I, const GhostRec& Rg, const double* 
         }
     }
     __syncwarp();
+    if (Rg.kind != BC_FAR_FIELD) {
+        const bool ok = __shfl_sync(0xffffffffu, lane == 0 ? (wall_outflow_vjp(I, Rg, G) ? 1 : 0) : 0, 0) != 0;
+        if (!ok) {
+            if (lane == 0) report(I, 1, 3, (unsigned)Rg.gid);
+            return;
+        }
+        __syncwarp();
+    } else {
     // u_k = R x_k: xb_k = R^T ub_k, Rb += ub_k x_k^T
     if (lane < 30) {
         const int k = lane / 6, m2 = lane - 6 * (lane / 6);
@@ -1126,6 +1288,7 @@ __device__ void ghost_vjp_warp(const Inst& I, const GhostRec& Rg, const double* 
         const double bu[6] = {b[0], b[1] * nx - b[2] * ny, b[1] * ny + b[2] * nx, b[3], b[4], b[5]};
         for (int c = 0; c < 6; ++c) atomicAdd(&pbar_k[c], bu[c]);
     }
+    } // FarField
     // v[k][c] = sum_r (alpha_r / sum) V_r^k -> V-bar, alpha-bar -> beta-bar,
     // lanes (c, r)
     const int oc = lane / 5, orr = lane - 5 * (lane / 5);
@@ -1203,7 +1366,7 @@ __global__ void __launch_bounds__(128) k_adj_ghost_tail(const Inst* __restrict__
     if (g >= nh) return;
     const GhostRec Rg = heavy[g];
     const Inst& I = insts[Rg.inst];
-    if (has_error(I) || Rg.kind != BC_FAR_FIELD) return;
+    if (has_error(I)) return;
     double q6[6];
     const Roe q = nearest_roe(I, Rg, Xb + I.aoff, q6);
     const double* o = slots + (size_t)g * AG_SLOT + AG_RB;
@@ -1237,7 +1400,7 @@ __global__ void __launch_bounds__(AG_WARPS * 32) k_adj_ghosts(const Inst* __rest
         if (g >= nh) return;
         const GhostRec Rg = heavy[g];
         const Inst& I = insts[Rg.inst];
-        if (has_error(I) || Rg.kind != BC_FAR_FIELD) return;
+        if (has_error(I)) return;
         ghost_vjp_warp(I, Rg, hrec + (size_t)Rg.heavy * GH_REC, Xb + I.aoff, Wb + I.aoff, Ubb + I.aoff,
                        pbar + 8 * Rg.inst, slots + (size_t)g * AG_SLOT, G[threadIdx.x >> 5], lane);
     } else {

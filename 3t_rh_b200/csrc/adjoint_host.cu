@@ -65,15 +65,6 @@ long long max_plane(const rh3t_ctx* c) {
     return m;
 }
 
-int check_supported(rh3t_ctx* c) {
-    for (int k = 0; k < c->n_inst; ++k)
-        if (c->hi[k].adj_unsupported)
-            return set_error(c, RH3T_ERR_INVALID_ARGUMENT,
-                             "adjoint: Wall and Outflow ghosts have no adjoint (FarField, ReflectiveWall, ZerothOrder, "
-                             "Periodic, Constant and TimeDependent do)");
-    return RH3T_OK;
-}
-
 // the work buffers every vjp needs (Y, U0, U1, U2, W, rbar, pbar, dtbar)
 int ensure_work(rh3t_ctx* c) {
     if (!c->adj) c->adj = new AdjBuffers();
@@ -136,7 +127,6 @@ int fetch_status(rh3t_ctx* c) { return rh3t_synchronize(c); }
 extern "C" int rh3t_l_vjp(rh3t_ctx* c, int32_t k, const double* rbar, double* ubar, double* pbar8) {
     if (!c || !rbar || !ubar) return RH3T_ERR_INVALID_ARGUMENT;
     if (k < 0 || k >= c->n_inst) return set_error(c, RH3T_ERR_INVALID_ARGUMENT, "instance index out of range");
-    if (int rc = check_supported(c)) return rc;
     CK(c, cudaSetDevice(c->device));
     if (int rc = ensure_work(c)) return rc;
     AdjBuffers* a = c->adj;
@@ -167,7 +157,6 @@ extern "C" int rh3t_l_vjp(rh3t_ctx* c, int32_t k, const double* rbar, double* ub
 
 extern "C" int rh3t_adjoint_forward(rh3t_ctx* c, int32_t nsteps, double cfl_factor, int32_t ckpt_every) {
     if (!c || nsteps <= 0 || ckpt_every <= 0) return RH3T_ERR_INVALID_ARGUMENT;
-    if (int rc = check_supported(c)) return rc;
     CK(c, cudaSetDevice(c->device));
     if (int rc = ensure_work(c)) return rc;
     AdjBuffers* a = c->adj;

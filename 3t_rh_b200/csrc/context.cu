@@ -296,7 +296,6 @@ int build_instance(const rh3t_instance& d, int inst, HostInst& H, Inst& I, Built
         R.ny = gt->proj[5 * g + 3]; R.dist = gt->proj[5 * g + 4];
         R.heavy = -1;
         const int kind = R.kind;
-        if (kind == BC_WALL || kind == BC_OUTFLOW) H.adj_unsupported = true;
         if (kind == BC_WALL || kind == BC_OUTFLOW || kind == BC_FAR_FIELD) {
             int k = gt->pre[g];
             if (k < 0 || k >= nh) {
@@ -701,6 +700,7 @@ extern "C" void rh3t_destroy(rh3t_ctx* c) {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    io_free(c);
     adj_free(c);
     if (c->graph) cudaGraphExecDestroy(c->graph);
     dfree(c->d_state); dfree(c->d_mask); dfree(c->d_faces); dfree(c->d_bcs); dfree(c->d_sc); dfree(c->d_err);

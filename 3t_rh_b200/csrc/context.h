@@ -26,7 +26,6 @@ struct HostInst {
     int gh0 = 0, ngh = 0, gc0 = 0, ngc = 0; // heavy / cheap segments of d_gpart
     int tx0 = 0, ntx = 0, ty0 = 0, nty = 0, tc0 = 0, ntc = 0, tr0 = 0, ntr = 0;
     int diffusion = 0;
-    bool adj_unsupported = false;  // has Wall or Outflow ghosts (no adjoint)
     Shape shape;
 };
 
@@ -65,6 +64,7 @@ struct rh3t_ctx {
     long long total_planes = 0;   // sum of 6*plane: size of a batch-wide plane set
     long long max_faces = 0;      // max over instances of max((nx+1)*ny, nx*(ny+1))
     struct AdjBuffers* adj = nullptr;
+    struct rh3t_io* io = nullptr; // snapshot and diagnostic buffers (io.cu)
     int n_ghosts = 0, n_heavy = 0, n_gheavy = 0, n_gcheap = 0, max_ghosts = 0;
     cudaGraphExec_t graph = nullptr;
     long long launches = 0;
@@ -83,6 +83,7 @@ void instance_tiles(const HostInst& H, const Shape& sh, int inst, std::vector<Ti
 void enqueue_flux(rh3t_ctx* c, cudaStream_t s, int stage, Span r);
 void enqueue_rhs(rh3t_ctx* c, cudaStream_t s, int stage, int mode, double* rhs, Span r);
 void adj_free(rh3t_ctx* c);
+void io_free(rh3t_ctx* c);
 } // namespace rh3t
 
 #define CK(ctx, call)                                                  \

@@ -95,11 +95,13 @@ template <int N> __device__ __forceinline__ DualN<N> operator/(double a, const D
     return r;
 }
 
+// at a.v = 0 a direction with zero tangent keeps a zero derivative (the
+// local dt's discriminant is exactly 0 when both exchange coefficients are)
 template <int N> __device__ __forceinline__ DualN<N> sqrt(const DualN<N>& a) {
     const double s = ::sqrt(a.v), h = 0.5 / s;
     DualN<N> r(s);
 #pragma unroll
-    for (int k = 0; k < N; ++k) r.d[k] = a.d[k] * h;
+    for (int k = 0; k < N; ++k) r.d[k] = a.d[k] == 0.0 ? 0.0 : a.d[k] * h;
     return r;
 }
 template <int N> __device__ __forceinline__ DualN<N> fabs(const DualN<N>& a) { return a.v < 0.0 ? -a : a; }

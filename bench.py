@@ -395,8 +395,7 @@ def run_batch(args, rh, flops, torch, dist, world, rank, local):
         for _ in range(k_e2e):
             b.upload_values(host, times)
             b.advance(1, CFL)
-            v2, times = b.download_values()
-            host[:] = v2
+            b.download_values(out=host, times=times)
         el = time.perf_counter() - t0
         nb = host.size * 8
         e2e = {"value": world * cells * k_e2e / el, "unit": "cell-updates/s", "h2d_bytes_per_step": nb + 8 * b.n,

@@ -247,13 +247,14 @@ int rh3t_autotune(rh3t_ctx* ctx, const char* cache_path, int32_t reps, rh3t_tune
 
 /* Adjoint (no reference counterpart: the reference has no derivative
  * code). Hand-written vector-Jacobian products of l() and of the SSP-RK3
- * step, for instances whose ghosts are FarField, ReflectiveWall, ZerothOrder,
- * Periodic, Constant or TimeDependent (Wall and Outflow are rejected with
- * RH3T_ERR_INVALID_ARGUMENT). Kinks follow the values: d|x|/dx = +1 at 0,
- * max/min pass the derivative to the first argument on ties, FarField rows
- * switch on lambda < 0, dt's derivative goes to the first minimising cell.
- * Parameter cotangents per instance (8 doubles): the FarField state (6, one
- * for all FarField sides), omega_ei, omega_er. */
+ * step, for every BC kind (Wall: both ILW solves in reverse; Outflow: the
+ * LODI row). Kinks follow the values: d|x|/dx = +1 at 0, max/min pass the
+ * derivative to the first argument on ties, FarField rows switch on
+ * lambda < 0, the Outflow row on lambda_1 < 0, dt's derivative goes to the
+ * first minimising cell. Parameter cotangents per instance (8 doubles): the
+ * FarField state (6, one for all FarField sides), omega_ei, omega_er (the
+ * Outflow p_inf, sigma, l_domain and Constant / TimeDependent states are
+ * held fixed). */
 /* rbar: nx*ny*6 cotangent of l()'s result for instance k; ubar (out): the
  * cotangent of the resident state, pbar8 (out, may be NULL). */
 int rh3t_l_vjp(rh3t_ctx* ctx, int32_t k, const double* rbar, double* ubar, double* pbar8);
@@ -267,6 +268,28 @@ int rh3t_adjoint_forward(rh3t_ctx* ctx, int32_t nsteps, double cfl_factor, int32
  * segment from its checkpoint; the resident states are those at the end of
  * the forward run afterwards. */
 int rh3t_adjoint_backward(rh3t_ctx* ctx, const double* dJ_du, double* dJ_du0, double* dJ_dparams);
+
+/* io.rs:25-99 save_data: instance k's resident state as an RH3TBIN1 file
+ * (header: "RH3TBIN1", u32 version 1, u32 nvar 8, u64 nx, u64 ny, f64 time;
+ * payload j-major / i-fastest, per node f64 x, y, rho, mom_x, mom_y, ee, ei,
+ * er, the state NaN at non-fluid nodes; little endian). The payload is packed
+ * on the device and copied to pinned host memory on the context's stream; a
+ * host thread writes `path`.tmp and renames it to `path`, so the call
+ * returns before the file is written. The next rh3t_snapshot or
+ * rh3t_snapshot_wait joins that write and returns its status. */
+int rh3t_snapshot(rh3t_ctx* ctx, int32_t k, const char* path);
+int rh3t_snapshot_wait(rh3t_ctx* ctx);
+/* io.rs:101-123 load_data: instance k's state and time from an RH3TBIN1
+ * file; the header must match (magic, version, nvar, nx, ny) and every fluid
+ * node's state must be finite (RH3T_ERR_INVALID_ARGUMENT with the
+ * reference's message otherwise). */
+int rh3t_restart(rh3t_ctx* ctx, int32_t k, const char* path);
+/* py_utils/energy_split.py as a device reduction over instance k's fluid
+ * nodes: out[0..2] max |ee - ei|, |ee - er|, |ei - er|; out[3..5] their
+ * means; out[6..8] their root mean squares; out[9], out[10] (x, y) of the
+ * first node (j-major order) of the maximum |ee - er|; out[11] the number of
+ * fluid nodes. */
+int rh3t_energy_split(rh3t_ctx* ctx, int32_t k, double* out);
 
 /* Field::value host <-> device (values of non-fluid cells are ignored on
  * upload and returned as 0 on download), plus Field::time. */
