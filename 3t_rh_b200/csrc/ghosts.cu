@@ -13,8 +13,11 @@
 // k_ghosts, heavy ghosts on persistent warps, one ghost at a time per warp.
 // A ghost's record (S_r, w, d, the E_r stencil and this stage's L, R,
 // lambda; 10.5 KB) arrives in shared memory by one bulk copy (cp.async.bulk,
-// completion on an mbarrier) issued one ghost ahead, so the table stream
-// overlaps the arithmetic. Per ghost:
+// completion on an mbarrier). One record buffer per warp: L, R and lambda
+// are copied out of it first, and once step 4 has read S_r, w and d the
+// next ghost's copy is issued into the same buffer, so the table stream
+// overlaps steps 5-6 and the next ghost's gather, and 12 warps fit on an SM.
+// Per ghost:
 //   1. every lane gathers its E_r stencil nodes (E_0..E_4, 55 nodes), one
 //      ghost ahead (the loads of the next ghost are in flight meanwhile);
 //   2. lanes spread over the 55 stencil nodes: rotate the momentum and
@@ -41,7 +44,7 @@
 namespace rh3t {
 
 constexpr int GH_WARPS = 4;
-constexpr int GH_BLOCKS_PER_SM = 2;
+constexpr int GH_BLOCKS_PER_SM = 3;
 constexpr int GH_PREP_THREADS = 128;
 constexpr int GH_WAIT_LIMIT = 1 << 20; // try_wait rounds before a wait counts as timed out
 constexpr int GH_TIMEOUT_CODE = 11;    // RH3T_ERR_DEVICE_TIMEOUT
@@ -57,7 +60,8 @@ __constant__ unsigned char kVItem[32] = {
     0x12, 0xff, 0xff, 0xff, 0x19, 0x08, 0xff, 0xff, 0xff, 0x1a, 0x09, 0xff, 0xff, 0xff, 0x20, 0x21};
 
 struct GhostWarp {
-    double rec[2][GH_REC]; // double-buffered heavy records
+    double rec[1][GH_REC]; // the heavy record (the next one is copied in during step 5)
+    double LR[80];         // this ghost's L, R, lambda (copied out of the record)
     double D[56][6];       // characteristic data d_c at stencil node a
     double ACC[56][6];     // (S_r d_c) at stencil row a; later u[5][6] and vinf[6]
     double alpha[6][5];
@@ -338,14 +342,15 @@ __device__ __forceinline__ void acc_row(GhostWarp& G, const double* __restrict__
 
 __device__ __forceinline__ void heavy_ghost(const Inst& I, const GhostRec& Rg, GhostWarp& G,
                                             const double* __restrict__ rec, int lane, int stage, int row1, int row2,
-                                            unsigned vitem, const double s0[6], const double s1[6]) {
+                                            unsigned vitem, const double s0[6], const double s1[6],
+                                            const double* next_rec) {
     const DevParams& P = I.P;
     double* buf = const_cast<double*>(stage_src(I, stage));
     const long long plane = I.plane;
     const double nx = Rg.nx, ny = Rg.ny;
-    const double* L = rec + GH_L;
-    const double* Rc = rec + GH_R;
-    const double* lam = rec + GH_LAM;
+    const double* L = G.LR;
+    const double* Rc = G.LR + GH_LR_R;
+    const double* lam = G.LR + GH_LR_LAM;
     // 2. characteristic data of the 55 stencil nodes
     project_node(G, L, s0, nx, ny, lane);
     if (lane + 32 < 55) project_node(G, L, s1, nx, ny, lane + 32);
@@ -380,6 +385,8 @@ __device__ __forceinline__ void heavy_ghost(const Inst& I, const GhostRec& Rg, G
         for (int c = 0; c < 6; ++c) G.V[c][r * (r + 1) / 2 + k] = v[c];
     }
     __syncwarp();
+    // the record is not read below: bring in the next ghost's
+    if (lane == 0 && next_rec) bulk_load(G.rec[0], next_rec, GH_REC * 8, &G.bar[0]);
     // 5. nonlinear weights (bc1.rs:247-252); V^(k)_r = 0 for k > r
     if (lane < 30) {
         const int k = lane / 6, c = lane - 6 * (lane / 6);
@@ -415,7 +422,7 @@ __device__ __forceinline__ void heavy_ghost(const Inst& I, const GhostRec& Rg, G
             u[k][i] = acc;
         }
     } else if (lane == 0) {
-        ok = serial_tail(I, Rg, rec + GH_L, G.v, u);
+        ok = serial_tail(I, Rg, G.LR, G.v, u);
     }
     __syncwarp();
     ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
@@ -450,7 +457,7 @@ __device__ __forceinline__ void gather_stencil(const Inst& I, const double* __re
 }
 
 // warps take the heavy ghosts in turn (record of the next one in flight)
-__global__ void __launch_bounds__(GH_WARPS * 32) k_ghosts(const Inst* __restrict__ insts,
+__global__ void __launch_bounds__(GH_WARPS * 32, GH_BLOCKS_PER_SM) k_ghosts(const Inst* __restrict__ insts,
                                                          const GhostRec* __restrict__ heavy, int nh,
                                                          const double* __restrict__ hrec, int stage) {
     extern __shared__ __align__(128) unsigned char gh_smem[];
@@ -469,7 +476,6 @@ __global__ void __launch_bounds__(GH_WARPS * 32) k_ghosts(const Inst* __restrict
         const unsigned vitem = kVItem[lane];
         if (lane == 0) {
             mbar_init(&G.bar[0]);
-            mbar_init(&G.bar[1]);
             mbar_fence_init();
             bulk_load(G.rec[0], hrec + (size_t)heavy[g].heavy * GH_REC, GH_REC * 8, &G.bar[0]);
         }
@@ -482,10 +488,8 @@ __global__ void __launch_bounds__(GH_WARPS * 32) k_ghosts(const Inst* __restrict
             gather_stencil(insts[R0.inst], hrec + (size_t)R0.heavy * GH_REC, lane, stage, s0, s1);
         }
         for (int it = 0; g < nh; ++it, g += stride) {
-            const int b = it & 1;
             const int gn = g + stride;
-            if (lane == 0 && gn < nh)
-                bulk_load(G.rec[b ^ 1], hrec + (size_t)heavy[gn].heavy * GH_REC, GH_REC * 8, &G.bar[b ^ 1]);
+            const double* next_rec = gn < nh ? hrec + (size_t)heavy[gn].heavy * GH_REC : nullptr;
             const GhostRec Rg = heavy[g];
             const Inst& I = insts[Rg.inst];
             const bool skip = has_error(I);
@@ -494,13 +498,15 @@ __global__ void __launch_bounds__(GH_WARPS * 32) k_ghosts(const Inst* __restrict
                 const GhostRec& Rn = heavy[gn];
                 gather_stencil(insts[Rn.inst], hrec + (size_t)Rn.heavy * GH_REC, lane, stage, n0, n1);
             }
-            const bool ok = __all_sync(0xffffffffu, mbar_wait(&G.bar[b], (uint32_t)((it >> 1) & 1)));
+            const bool ok = __all_sync(0xffffffffu, mbar_wait(&G.bar[0], (uint32_t)(it & 1)));
             if (!ok) {
                 if (lane == 0) report(I, 1 + 2 * stage, GH_TIMEOUT_CODE, (unsigned)Rg.gid);
-                if (gn < nh) mbar_wait(&G.bar[b ^ 1], (uint32_t)(((it + 1) >> 1) & 1)); // drain the prefetch
                 return;
             }
-            if (!skip) heavy_ghost(I, Rg, G, G.rec[b], lane, stage, row1, row2, vitem, s0, s1);
+            for (int e = lane; e < GH_LR; e += 32) G.LR[e] = G.rec[0][GH_L + e];
+            __syncwarp();
+            if (!skip) heavy_ghost(I, Rg, G, G.rec[0], lane, stage, row1, row2, vitem, s0, s1, next_rec);
+            else if (lane == 0 && next_rec) bulk_load(G.rec[0], next_rec, GH_REC * 8, &G.bar[0]);
             __syncwarp();
 #pragma unroll
             for (int q = 0; q < 6; ++q) { s0[q] = n0[q]; s1[q] = n1[q]; }
