@@ -1135,7 +1135,10 @@ __device__ __forceinline__ void prefetch_record_l2(const double* rec) {
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(rec), "r"((unsigned)(GH_REC * 8)) : "memory");
 }
 
-// one heavy (FarField) ghost per warp; gb from W at the ghost node
+// one heavy ghost per warp; gb from W at the ghost node. WO: the Wall /
+// Outflow instantiation (their rows on one lane through wall_outflow_vjp);
+// the FarField one has no call and keeps its registers
+template <bool WO>
 __device__ void ghost_vjp_warp(const Inst& I, const GhostRec& Rg, const double* __restrict__ rec,
                                const double* __restrict__ X, const double* __restrict__ W, double* __restrict__ Ub,
                                double* __restrict__ pbar_k, double* __restrict__ slot, AdjGhostWarp& G, int lane) {
@@ -1244,7 +1247,7 @@ __device__ void ghost_vjp_warp(const Inst& I, const GhostRec& Rg, const double* 
         }
     }
     __syncwarp();
-    if (Rg.kind != BC_FAR_FIELD) {
+    if (WO) {
         const bool ok = __shfl_sync(0xffffffffu, lane == 0 ? (wall_outflow_vjp(I, Rg, G) ? 1 : 0) : 0, 0) != 0;
         if (!ok) {
             if (lane == 0) report(I, 1, 3, (unsigned)Rg.gid);
@@ -1385,7 +1388,8 @@ __global__ void __launch_bounds__(128) k_adj_ghost_tail(const Inst* __restrict__
     atomic_add6(Ubb + I.aoff, I.plane, Rg.src, sb);
 }
 
-__global__ void __launch_bounds__(AG_WARPS * 32) k_adj_ghosts(const Inst* __restrict__ insts,
+template <bool WO>
+__global__ void __launch_bounds__(AG_WARPS * 32, 5) k_adj_ghosts(const Inst* __restrict__ insts,
                                                              const GhostRec* __restrict__ heavy, int nh,
                                                              const GhostRec* __restrict__ cheap, int nc,
                                                              const double* __restrict__ hrec,
@@ -1400,8 +1404,8 @@ __global__ void __launch_bounds__(AG_WARPS * 32) k_adj_ghosts(const Inst* __rest
         if (g >= nh) return;
         const GhostRec Rg = heavy[g];
         const Inst& I = insts[Rg.inst];
-        if (has_error(I)) return;
-        ghost_vjp_warp(I, Rg, hrec + (size_t)Rg.heavy * GH_REC, Xb + I.aoff, Wb + I.aoff, Ubb + I.aoff,
+        if (has_error(I) || (Rg.kind != BC_FAR_FIELD) != WO) return;
+        ghost_vjp_warp<WO>(I, Rg, hrec + (size_t)Rg.heavy * GH_REC, Xb + I.aoff, Wb + I.aoff, Ubb + I.aoff,
                        pbar + 8 * Rg.inst, slots + (size_t)g * AG_SLOT, G[threadIdx.x >> 5], lane);
     } else {
         const int g = (blockIdx.x - nbh) * (AG_WARPS * 32) + threadIdx.x;
@@ -1444,7 +1448,7 @@ __global__ void k_adj_fluid(const Inst* __restrict__ insts, int k0, const double
 void launch_adj_l(cudaStream_t s, const Inst* insts, int k0, int n, long long max_cells, const Tile* tx, int ntx,
                   const Tile* ty, int nty, const Tile* tr, int ntr, const GhostRec* heavy, int nh,
                   const GhostRec* cheap, int nc, const double* hrec, const double* X, const double* rbar, double* W,
-                  double* Ub, double* pbar, double* slots) {
+                  double* Ub, double* pbar, double* slots, int wall_outflow) {
     if (n <= 0) return;
     static bool attr = false;
     if (!attr) {
@@ -1462,13 +1466,17 @@ void launch_adj_l(cudaStream_t s, const Inst* insts, int k0, int n, long long ma
     if (ntr > 0) k_adj_cells<<<ntr, RHS_THREADS, ADJ_CELL_SMEM, s>>>(insts, tr, ntr, X, rbar, W, pbar);
     const int nbh = (nh + AG_WARPS - 1) / AG_WARPS, nbc = (nc + AG_WARPS * 32 - 1) / (AG_WARPS * 32);
     if (nbh + nbc > 0)
-        k_adj_ghosts<<<nbh + nbc, AG_WARPS * 32, 0, s>>>(insts, heavy, nh, cheap, nc, hrec, X, W, Ub, pbar, slots,
-                                                          nbh);
+        k_adj_ghosts<false><<<nbh + nbc, AG_WARPS * 32, 0, s>>>(insts, heavy, nh, cheap, nc, hrec, X, W, Ub, pbar,
+                                                                 slots, nbh);
+    if (wall_outflow && nbh > 0)
+        k_adj_ghosts<true><<<nbh, AG_WARPS * 32, 0, s>>>(insts, heavy, nh, cheap, 0, hrec, X, W, Ub, pbar, slots, nbh);
     if (nh > 0) k_adj_ghost_tail<<<(nh + 127) / 128, 128, 0, s>>>(insts, heavy, nh, X, slots, Ub);
     k_adj_fluid<<<dim3(cb, n), 128, 0, s>>>(insts, k0, W, Ub);
 }
 
-int adj_l_launches(int nh, int nc) { return 3 + (nh + nc > 0 ? 1 : 0) + (nh > 0 ? 2 : 0); }
+int adj_l_launches(int nh, int nc, int wall_outflow) {
+    return 3 + (nh + nc > 0 ? 1 : 0) + (nh > 0 ? 2 : 0) + (wall_outflow && nh > 0 ? 1 : 0);
+}
 
 // ---------------------------------------------------------------- RK3 step plumbing
 // copy the 6 planes of stage buffer `which` (0 U, 1 A, 2 B) of instances

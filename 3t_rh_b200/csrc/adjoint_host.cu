@@ -95,9 +95,11 @@ void enqueue_vjp_l(rh3t_ctx* c, const double* X, const double* rbar, double* Ub)
     cudaMemsetAsync(a->W, 0, (size_t)c->total_planes * sizeof(double), c->stream);
     int nh, nc;
     ghost_ranges(c, nh, nc);
+    int wo = 0;
+    for (const HostInst& H : c->hi) wo |= H.n_wall_outflow > 0;
     launch_adj_l(c->stream, c->d_inst, 0, c->n_inst, c->max_cells, c->d_tx, c->ntx, c->d_ty, c->nty, c->d_tr, c->ntr,
-                 c->d_gpart, nh, c->d_gpart + c->n_gheavy, nc, c->d_hrec, X, rbar, a->W, Ub, a->pbar, a->gslots);
-    c->launches += adj_l_launches(nh, nc);
+                 c->d_gpart, nh, c->d_gpart + c->n_gheavy, nc, c->d_hrec, X, rbar, a->W, Ub, a->pbar, a->gslots, wo);
+    c->launches += adj_l_launches(nh, nc, wo);
 }
 
 // forward stage with the adjoint's record (stage state with ghosts, rhs)

@@ -296,6 +296,7 @@ int build_instance(const rh3t_instance& d, int inst, HostInst& H, Inst& I, Built
         R.ny = gt->proj[5 * g + 3]; R.dist = gt->proj[5 * g + 4];
         R.heavy = -1;
         const int kind = R.kind;
+        if (kind == BC_WALL || kind == BC_OUTFLOW) ++H.n_wall_outflow;
         if (kind == BC_WALL || kind == BC_OUTFLOW || kind == BC_FAR_FIELD) {
             int k = gt->pre[g];
             if (k < 0 || k >= nh) {

@@ -26,6 +26,7 @@ struct HostInst {
     int gh0 = 0, ngh = 0, gc0 = 0, ngc = 0; // heavy / cheap segments of d_gpart
     int tx0 = 0, ntx = 0, ty0 = 0, nty = 0, tc0 = 0, ntc = 0, tr0 = 0, ntr = 0;
     int diffusion = 0;
+    int n_wall_outflow = 0;        // heavy ghosts of kind Wall or Outflow
     Shape shape;
 };
 

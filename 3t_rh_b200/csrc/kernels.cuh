@@ -29,8 +29,8 @@ constexpr int AG_SLOT = 120;
 void launch_adj_l(cudaStream_t s, const Inst* insts, int k0, int n, long long max_cells, const Tile* tx, int ntx,
                   const Tile* ty, int nty, const Tile* tr, int ntr, const GhostRec* heavy, int nh,
                   const GhostRec* cheap, int nc, const double* hrec, const double* X, const double* rbar, double* W,
-                  double* Ub, double* pbar, double* slots);
-int adj_l_launches(int nh, int nc);
+                  double* Ub, double* pbar, double* slots, int wall_outflow);
+int adj_l_launches(int nh, int nc, int wall_outflow);
 void launch_adj_copy(cudaStream_t s, const Inst* insts, int k0, int n, long long max_plane, int which, double* set,
                      int dir);
 void launch_adj_aos(cudaStream_t s, const Inst* insts, int k0, int n, long long max_cells, double* aos, double* set,
