@@ -662,13 +662,20 @@ class Batch(_SnapshotIO):
         """nsteps steps of every instance with checkpoints every ckpt_every."""
         self._check(self.L.rh3t_adjoint_forward(self.h, int(nsteps), float(cfl_factor), int(ckpt_every)))
 
-    def adjoint_backward(self, dJ_du):
+    def adjoint_backward(self, dJ_du, out=None):
         """dJ_du: per-instance list of (nx*ny x 6) arrays or their
-        concatenation. Returns ([dJ/du0 per instance], dJ/dparams (n x 8))."""
+        concatenation. Returns ([dJ/du0 per instance], dJ/dparams (n x 8));
+        out (total_cells x 6 float64, C-contiguous, e.g. pinned host memory)
+        receives dJ/du0 when given."""
         if isinstance(dJ_du, (list, tuple)):
             dJ_du = np.concatenate([_arr(x, np.float64).reshape(-1, 6) for x in dJ_du])
         lam = _arr(dJ_du, np.float64)
-        g0 = np.zeros((int(self.offsets[-1]), 6))
+        if out is None:
+            g0 = np.zeros((int(self.offsets[-1]), 6))
+        elif out.dtype != np.float64 or not out.flags.c_contiguous or out.size != int(self.offsets[-1]) * 6:
+            raise ValueError("out must be a C-contiguous float64 array of total_cells x 6")
+        else:
+            g0 = out
         gp = np.zeros((self.n, 8))
         self._check(self.L.rh3t_adjoint_backward(self.h, lam.ctypes.data, g0.ctypes.data, gp.ctypes.data))
         return [g0[self.offsets[k]:self.offsets[k + 1]] for k in range(self.n)], gp

@@ -40,14 +40,15 @@ struct AdjBuffers {
     double* dtbar = nullptr;    // n_inst
     unsigned long long* argmin = nullptr; // n_inst: the dt-minimising cell
     double* gslots = nullptr;   // AG_SLOT doubles per heavy ghost (ghost vjp scratch)
+    double* final_state = nullptr; // the forward run's end state, restored after the sweep
 };
 
 namespace rh3t {
 void adj_free(rh3t_ctx* c) {
     AdjBuffers* a = c->adj;
     if (!a) return;
-    void* ptrs[] = {a->ckpt, a->ckpt_sc, a->seg,  a->seg_sc, a->Y,     a->U0,    a->U1,
-                    a->U2,   a->W,       a->rbar, a->pbar,   a->dtbar, a->argmin, a->gslots};
+    void* ptrs[] = {a->ckpt, a->ckpt_sc, a->seg,   a->seg_sc, a->Y,      a->U0,     a->U1,
+                    a->U2,   a->W,       a->rbar,  a->pbar,   a->dtbar, a->argmin, a->gslots, a->final_state};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete a;
@@ -80,6 +81,7 @@ int ensure_work(rh3t_ctx* c) {
     CK(c, cudaMalloc(&a->dtbar, (size_t)c->n_inst * sizeof(double)));
     CK(c, cudaMalloc(&a->argmin, (size_t)c->n_inst * sizeof(unsigned long long)));
     CK(c, cudaMalloc(&a->gslots, (size_t)std::max(c->n_gheavy, 1) * AG_SLOT * sizeof(double)));
+    CK(c, cudaMalloc(&a->final_state, np * sizeof(double)));
     return RH3T_OK;
 }
 
@@ -229,8 +231,7 @@ extern "C" int rh3t_adjoint_backward(rh3t_ctx* c, const double* dJ_du, double* d
     std::vector<DevScalars> end_sc(ni);
     CK(c, cudaMemcpyAsync(end_sc.data(), c->d_sc, ni * sizeof(DevScalars), cudaMemcpyDeviceToHost, s));
     CK(c, cudaStreamSynchronize(s));
-    double* final_state = nullptr;
-    CK(c, cudaMalloc(&final_state, np * sizeof(double)));
+    double* final_state = a->final_state;
     launch_adj_copy(s, c->d_inst, 0, c->n_inst, mp, 0, final_state, 0);
     for (int q = a->n_ckpt - 1; q >= 0; --q) {
         const int len = std::min(a->ckpt_every, a->nsteps - q * a->ckpt_every);
@@ -280,7 +281,6 @@ extern "C" int rh3t_adjoint_backward(rh3t_ctx* c, const double* dJ_du, double* d
     CK(c, cudaMemcpyAsync(c->d_sc, end_sc.data(), ni * sizeof(DevScalars), cudaMemcpyHostToDevice, s));
     c->launches += 1;
     CK(c, cudaStreamSynchronize(s));
-    cudaFree(final_state);
     CK(c, cudaGetLastError());
     return fetch_status(c);
 }

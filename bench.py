@@ -171,12 +171,19 @@ def batch_oracle_rate(O, specs, budget_s, max_steps=None):
 
 
 def cpu_baseline(O, wl, budget_s=20.0, specs=None):
-    """The oracle (OpenMP, all host threads) on a bounded number of steps of the same workload."""
+    """The oracle (OpenMP, all host threads) on a bounded number of steps of the same workload,
+    and a short one-thread sample beside it."""
     if specs is not None:
+        threads = O.max_threads()
         v, n_inst, steps, el, build_s = batch_oracle_rate(O, specs, budget_s)
-        return {"value": v, "unit": "cell-updates/s", "cores": O.max_threads(), "kind": "port",
+        O.set_threads(1)
+        v1, n1, steps1, el1, _ = batch_oracle_rate(O, specs[:4], 3.0)
+        O.set_threads(threads)
+        return {"value": v, "unit": "cell-updates/s", "cores": threads, "kind": "port",
                 "sample": f"{steps} SSP-RK3 step(s) of each of the first {n_inst} of the {len(specs)} instances, "
-                          f"{el:.1f} s, after a {build_s:.1f} s ghost-grid build"}
+                          f"{el:.1f} s, after a {build_s:.1f} s ghost-grid build",
+                "one_core": {"value": v1, "cores": 1,
+                             "sample": f"{steps1} step(s) of the first {n1} instances, {el1:.1f} s"}}
     t0 = time.perf_counter()
     case = make_oracle(O, wl)
     build_s = time.perf_counter() - t0
@@ -272,17 +279,36 @@ def adjoint_bench(rh, torch, local, exact, nsteps=200, ckpt=20, n=32):
     _, f_ms, f_wall = timed(lambda: fwd.advance(nsteps, CFL), fwd)
     fwd.close()
     b = rh.Batch(fields, grids, device=local, exact=exact)
-    b.adjoint_forward(2, CFL, 2)  # warm-up: buffers, graph
+    # warm-up with the timed run's checkpoint layout: its buffers (checkpoints,
+    # the segment record) are allocated here, not inside the timed region
+    b.adjoint_forward(nsteps, CFL, ckpt)
     b.adjoint_backward([np.zeros((int(c), 6)) for c in b.cells])
     b.upload(fields)
 
+    # host buffers of the caller: pinned, as for any large device transfer
+    total = int(b.offsets[-1])
+    vals_h = torch.empty((total, 6), dtype=torch.float64, pin_memory=True).numpy()
+    lam_h = torch.empty((total, 6), dtype=torch.float64, pin_memory=True).numpy()
+    g0_h = torch.empty((total, 6), dtype=torch.float64, pin_memory=True).numpy()
+    times_h = np.zeros(b.n)
+    st = torch.cuda.ExternalStream(b.stream, device=dev)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+
     def adjoint():
+        ev[0].record(st)
         b.adjoint_forward(nsteps, CFL, ckpt)
-        res = b.download()
-        lam = [J.grad(u) for J, (u, _) in zip(Js, res)]
-        return res, b.adjoint_backward(lam)
+        ev[1].record(st)
+        b.download_values(out=vals_h, times=times_h)
+        for k, J in enumerate(Js):
+            o0, o1 = b.offsets[k], b.offsets[k + 1]
+            lam_h[o0:o1] = J.grad(vals_h[o0:o1])
+        ev[2].record(st)
+        out = b.adjoint_backward(lam_h, out=g0_h)
+        ev[3].record(st)
+        return [(vals_h[b.offsets[k]:b.offsets[k + 1]], times_h[k]) for k in range(b.n)], out
 
     (res, (g0, gp)), a_ms, a_wall = timed(adjoint, b)
+    lib_ms = ev[0].elapsed_time(ev[1]) + ev[2].elapsed_time(ev[3])
     dmach = []
     for k, sp in enumerate(specs):
         hm = 1e-7
@@ -293,6 +319,9 @@ def adjoint_bench(rh, torch, local, exact, nsteps=200, ckpt=20, n=32):
                         f"seed 20261203; J = surface pressure on the arc after {nsteps} steps; gradient in Mach, "
                         f"omega_ei, omega_er and the initial state; checkpoints every {ckpt} steps",
             "forward_ms": f_ms, "adjoint_ms": a_ms, "adj_fwd_ratio": a_ms / f_ms,
+            "adjoint_library_ms": lib_ms, "adj_fwd_ratio_library": lib_ms / f_ms,
+            "ratio_note": "adjoint_ms: checkpointed forward + download + host objective gradient + reverse sweep; "
+                          "adjoint_library_ms: rh3t_adjoint_forward + rh3t_adjoint_backward only",
             "wall_ms": {"forward": f_wall, "adjoint": a_wall},
             "J_first": float(Js[0].value(res[0][0])), "dJ_dMach_first": dmach[0],
             "dJ_domega_first": [float(gp[0, 6]), float(gp[0, 7])]}
