@@ -38,6 +38,12 @@ def _raise_last(L, h, rc):
     raise RH3TError(e.code or rc, e.message.decode(), e.stage, e.step, e.i, e.j, e.ghost, e.instance)
 
 
+def _raise_create(L, rc, what):
+    msg = C.create_string_buffer(192)
+    code = L.rh3t_create_error(msg, 192)
+    raise RH3TError(code or rc, f"{what}: {msg.value.decode()}" if msg.value else what)
+
+
 def _arr(a, dtype):
     return np.ascontiguousarray(a, dtype=dtype)
 
@@ -432,7 +438,7 @@ class Solver(_SnapshotIO):
                                 C.addressof(obc), len(field.bc_inner), C.addressof(ibc), C.byref(table), device,
                                 C.byref(h))
         if rc:
-            raise RH3TError(rc, "rh3t_create failed")
+            _raise_create(self.L, rc, "rh3t_create failed")
         self.h = h
         self.upload(field)
 
@@ -542,7 +548,7 @@ class Batch(_SnapshotIO):
         h = C.c_void_p()
         rc = self.L.rh3t_batch_create(self.n, C.addressof(desc), device, C.byref(h))
         if rc:
-            raise RH3TError(rc, "rh3t_batch_create failed")
+            _raise_create(self.L, rc, "rh3t_batch_create failed")
         self.h = h
         self.upload(fields)
 

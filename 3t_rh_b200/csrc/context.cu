@@ -519,22 +519,46 @@ extern "C" void rh3t_default_params(rh3t_params* p) {
     *p = rh3t_params{1.4, 1.4, 1.4, 1.0, 1.0, 1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.5, 10.0, 1e-12, 0.5};
 }
 
+// the failure of the last rh3t_batch_create / rh3t_create on this thread (the
+// context it would have returned no longer exists to carry it)
+static thread_local int g_create_code = 0;
+static thread_local char g_create_msg[192] = {0};
+
+static void set_create_error(int code, const char* m) {
+    g_create_code = code;
+    std::snprintf(g_create_msg, sizeof(g_create_msg), "%s", m ? m : "");
+}
+
+extern "C" int rh3t_create_error(char* message, int32_t len) {
+    if (message && len > 0) std::snprintf(message, (size_t)len, "%s", g_create_msg);
+    return g_create_code;
+}
+
 extern "C" int rh3t_batch_create(int32_t n, const rh3t_instance* desc, int32_t device, rh3t_ctx** out) {
+    set_create_error(0, "");
     if (!out) return RH3T_ERR_INVALID_ARGUMENT;
     *out = nullptr;
     if (n <= 0 || !desc) return RH3T_ERR_INVALID_ARGUMENT;
     for (int k = 0; k < n; ++k) { // argument checks come before any device call
         const rh3t_instance& d = desc[k];
         if (!d.grid || !d.params || !d.fluid || !d.ghosts || d.grid->nx <= 0 || d.grid->ny <= 0 ||
-            d.n_outer_bc < 0 || d.n_inner_bc < 0 || (d.n_outer_bc && !d.outer_bcs) || (d.n_inner_bc && !d.inner_bcs))
+            d.n_outer_bc < 0 || d.n_inner_bc < 0 || (d.n_outer_bc && !d.outer_bcs) || (d.n_inner_bc && !d.inner_bcs)) {
+            char m[96];
+            std::snprintf(m, sizeof(m), "instance %d: missing or malformed description", k);
+            set_create_error(RH3T_ERR_INVALID_ARGUMENT, m);
             return RH3T_ERR_INVALID_ARGUMENT;
+        }
     }
     int ndev = 0;
-    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || ndev <= device) return RH3T_ERR_NO_DEVICE;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || ndev <= device) {
+        set_create_error(RH3T_ERR_NO_DEVICE, "no such CUDA device");
+        return RH3T_ERR_NO_DEVICE;
+    }
     rh3t_ctx* c = new rh3t_ctx();
     c->device = device;
     auto fail = [&](int code, const char* m) {
         set_error(c, code, m);
+        set_create_error(code, m);
         std::fprintf(stderr, "rh3t_batch_create: %s\n", m);
         rh3t_destroy(c);
         return code;

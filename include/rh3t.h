@@ -359,6 +359,11 @@ int rh3t_math_check(int32_t device, const double* x, int32_t n, double q, double
 
 int rh3t_synchronize(rh3t_ctx* ctx);
 int rh3t_last_error(const rh3t_ctx* ctx, rh3t_error* out);
+/* status of the last rh3t_create / rh3t_batch_create on the calling thread
+ * (0 when it succeeded) and its message (the reference's panic text, e.g.
+ * "instance 1: periodic wrapped point is not fluid"; bc1.rs:594-604); the
+ * failed call returned no context to ask with rh3t_last_error. */
+int rh3t_create_error(char* message, int32_t len);
 /* number of kernels this context launched since creation (instrumentation) */
 int64_t rh3t_kernel_launches(const rh3t_ctx* ctx);
 /* the CUDA stream the context runs on (cudaStream_t) */
