@@ -14,21 +14,23 @@
 // A ghost's record (S_r, w, d, the E_r stencil and this stage's L, R,
 // lambda; 10.5 KB) arrives in shared memory by one bulk copy (cp.async.bulk,
 // completion on an mbarrier). One record buffer per warp: L, R and lambda
-// are copied out of it first, and once step 4 has read S_r, w and d the
-// next ghost's copy is issued into the same buffer, so the table stream
-// overlaps steps 5-6 and the next ghost's gather, and 12 warps fit on an SM.
+// are copied out of it first, and once step 3 has read S_r and w (and d is
+// in registers) the next ghost's copy is issued into the same buffer, so the
+// table stream overlaps steps 4-6, and 12 warps fit on an SM.
 // Per ghost:
-//   1. every lane gathers its E_r stencil nodes (E_0..E_4, 55 nodes), one
-//      ghost ahead (the loads of the next ghost are in flight meanwhile);
+//   1. the E_r stencil states (E_0..E_4, 55 nodes, two per lane) were
+//      gathered while the ghost before was processed; the fetches for the
+//      next ghost are spread over the steps so that none waits on another;
 //   2. lanes spread over the 55 stencil nodes: rotate the momentum and
 //      project on the six characteristic fields (bc1.rs:209-219);
-//   3. lanes spread over the 55 rows of S_0..S_4: (S_r d_c)_a for all six c,
-//      summed over b in order (bc1.rs:224-229); S_r is stored transposed so
-//      the lanes of one order read consecutive words;
-//   4. lanes (c, r): beta_{c,r} = sum_a d_a (S d)_a and
-//      alpha = d_r / (eps + beta)^q; lanes (r, k), placed on the lanes whose
-//      beta is short: V^(k)_{c,r} = w_{r,k} . d_c for all six c
-//      (bc1.rs:221-244);
+//   3. the 70 dot products with the stencil data, all six fields at once,
+//      in three slots of 25, 16 and 4 terms (a fixed per-lane schedule):
+//      the 55 rows of S_0..S_4, each stored as its beta term
+//      d_c,a (S_r d_c)_a, and the 15 rows w_{r,k}, V^(k)_{c,r} = w_{r,k} . d_c
+//      (bc1.rs:221-244); S_r is stored transposed so the lanes of one order
+//      read consecutive words;
+//   4. lanes (c, r): beta_{c,r} = the sum of its row terms in order and
+//      alpha = d_r / (eps + beta)^q;
 //   5. lanes (k, c): V^(k)_c = sum_r alpha_r / sum(alpha) V_r (bc1.rs:247-252);
 //   6. FarField rows, R products and the Taylor sum on lanes (bc1.rs:829-923);
 //      Wall (two 6x6 LU solves) and Outflow (LODI) on lane 0 (bc1.rs:691-828).
@@ -52,18 +54,47 @@ __constant__ int kStOff[6] = {0, 1, 5, 14, 30, 55};
 __constant__ int kSOff[6] = {0, 1, 17, 98, 354, 979};
 __constant__ int kWOff[6] = {0, 1, 9, 36, 100, 225};
 
-// Step 4 V items (r << 3 | k) per lane, 0xff for none: the 15 dot products
-// w_{r,k} . d (all six fields at once), longest on the lanes whose own beta
-// is shortest (lane c * 5 + r computes beta_{c,r}; lanes 30, 31 have none).
-__constant__ unsigned char kVItem[32] = {
-    0x22, 0x1b, 0x00, 0xff, 0xff, 0x23, 0x10, 0xff, 0xff, 0xff, 0x24, 0x11, 0xff, 0xff, 0xff, 0x18,
-    0x12, 0xff, 0xff, 0xff, 0x19, 0x08, 0xff, 0xff, 0xff, 0x1a, 0x09, 0xff, 0xff, 0xff, 0x20, 0x21};
+// Row of D holding stencil node a of order r: the order blocks start at
+// kDOff[r], whose residues mod 8 differ, so the 16-byte loads of D rows of
+// different orders at the same position fall in different banks.
+__constant__ int kDOff[5] = {0, 1, 5, 14, 31};
+__host__ __device__ constexpr int d_row(int a) { return a + (a >= 30 ? 1 : 0); }
+
+// Step 3 schedule: the 70 dot products with the stencil data d (55 rows of
+// S_0..S_4 and the 15 rows w_{r,k}), all six fields at once, as 35 pairs of
+// rows of one order (one load of a D row serves both), in two slots a warp
+// runs one after the other (25 and 4 terms at most). Row code:
+// w-row flag << 8 | r << 5 | a (S row) or k (w row); 0xffff = none.
+constexpr unsigned short kRowNone = 0xffff;
+__host__ __device__ constexpr unsigned short srow(int r, int a) { return (unsigned short)((r << 5) | a); }
+__host__ __device__ constexpr unsigned short wrow(int r, int k) { return (unsigned short)(0x100 | (r << 5) | k); }
+__host__ __device__ constexpr unsigned pair(unsigned short x, unsigned short y) { return (unsigned)x | ((unsigned)y << 16); }
+constexpr unsigned kPairNone = 0xffffffffu;
+__constant__ unsigned kSlotA[32] = {  // orders 4 (lanes 0-14), 3 (15-24), 2 (25-30), 1 (31)
+    pair(srow(4, 0), srow(4, 1)), pair(srow(4, 2), srow(4, 3)), pair(srow(4, 4), srow(4, 5)),
+    pair(srow(4, 6), srow(4, 7)), pair(srow(4, 8), srow(4, 9)), pair(srow(4, 10), srow(4, 11)),
+    pair(srow(4, 12), srow(4, 13)), pair(srow(4, 14), srow(4, 15)), pair(srow(4, 16), srow(4, 17)),
+    pair(srow(4, 18), srow(4, 19)), pair(srow(4, 20), srow(4, 21)), pair(srow(4, 22), srow(4, 23)),
+    pair(srow(4, 24), wrow(4, 0)), pair(wrow(4, 1), wrow(4, 2)), pair(wrow(4, 3), wrow(4, 4)),
+    pair(srow(3, 0), srow(3, 1)), pair(srow(3, 2), srow(3, 3)), pair(srow(3, 4), srow(3, 5)),
+    pair(srow(3, 6), srow(3, 7)), pair(srow(3, 8), srow(3, 9)), pair(srow(3, 10), srow(3, 11)),
+    pair(srow(3, 12), srow(3, 13)), pair(srow(3, 14), srow(3, 15)), pair(wrow(3, 0), wrow(3, 1)),
+    pair(wrow(3, 2), wrow(3, 3)),
+    pair(srow(2, 0), srow(2, 1)), pair(srow(2, 2), srow(2, 3)), pair(srow(2, 4), srow(2, 5)),
+    pair(srow(2, 6), srow(2, 7)), pair(srow(2, 8), wrow(2, 0)), pair(wrow(2, 1), wrow(2, 2)),
+    pair(srow(1, 0), srow(1, 1))};
+__constant__ unsigned kSlotB[32] = {  // the rest of order 1, order 0
+    pair(srow(1, 2), srow(1, 3)), pair(wrow(1, 0), wrow(1, 1)), pair(srow(0, 0), wrow(0, 0)),
+    kPairNone, kPairNone, kPairNone, kPairNone, kPairNone, kPairNone, kPairNone, kPairNone, kPairNone,
+    kPairNone, kPairNone, kPairNone, kPairNone, kPairNone, kPairNone, kPairNone, kPairNone, kPairNone,
+    kPairNone, kPairNone, kPairNone, kPairNone, kPairNone, kPairNone, kPairNone, kPairNone, kPairNone,
+    kPairNone, kPairNone};
 
 struct GhostWarp {
     double rec[1][GH_REC]; // the heavy record (the next one is copied in during step 5)
     double LR[80];         // this ghost's L, R, lambda (copied out of the record)
-    double D[56][6];       // characteristic data d_c at stencil node a
-    double ACC[56][6];     // (S_r d_c) at stencil row a; later u[5][6] and vinf[6]
+    double D[56][6];       // characteristic data d_c at stencil node a, row d_row(a)
+    double ACC[56][6];     // d_c,a (S_r d_c)_a at stencil row a; later u[5][6] and vinf[6]
     double alpha[6][5];
     double V[6][15];       // [c][r (r + 1) / 2 + k], k <= r
     double v[5][6];        // V^(k)_c
@@ -111,10 +142,6 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, uint32_t pari
         if (done) return true;
     }
     return false;
-}
-
-__device__ __forceinline__ int row_order(int R) {
-    return R < 1 ? 0 : (R < 5 ? 1 : (R < 14 ? 2 : (R < 30 ? 3 : 4)));
 }
 
 // bc1.rs:467-469 solve6 with LAPACK getrf/getrs semantics
@@ -320,30 +347,72 @@ __device__ __forceinline__ void project_node(GhostWarp& G, const double* __restr
     for (int c = 0; c < 6; ++c)
         d[c] = L[6 * c + 0] * u6[0] + L[6 * c + 1] * u6[1] + L[6 * c + 2] * u6[2] + L[6 * c + 3] * u6[3] +
                L[6 * c + 4] * u6[4] + L[6 * c + 5] * u6[5];
-    store_d6(G.D[a], d);
+    store_d6(G.D[d_row(a)], d);
 }
 
-// row R of S_r d_c for all six c (S_r transposed in the record)
-__device__ __forceinline__ void acc_row(GhostWarp& G, const double* __restrict__ rec, int R) {
-    const int r = row_order(R);
-    const int m = (r + 1) * (r + 1), off = kStOff[r], a = R - off;
-    const double* __restrict__ St = rec + GH_S + kSOff[r] + a;
-    double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-#pragma unroll 5
-    for (int b = 0; b < m; ++b) {
-        const double sv = St[b * m];
-        double d[6];
-        load_d6(G.D[off + b], d);
+// source of a step-3 row: S_r transposed in the record (stride m, so the
+// lanes of one order read consecutive words), or w_{r,k} (stride 1)
+__device__ __forceinline__ const double* row_src(const double* __restrict__ rec, unsigned code, int m, int& stride) {
+    const bool wr = (code >> 8) != 0;
+    const int r = (int)((code >> 5) & 7u), ix = (int)(code & 31u);
+    stride = wr ? 1 : m;
+    return wr ? rec + GH_W + kWOff[r] + ix * m : rec + GH_S + kSOff[r] + ix;
+}
+
+// an S row stores d_c,a (S_r d_c)_a, the term of beta_{c,r}; a w row stores
+// V^(k)_{c,r} = w_{r,k} . d_c
+__device__ __forceinline__ void row_out(GhostWarp& G, unsigned code, const double acc[6]) {
+    const int r = (int)((code >> 5) & 7u), ix = (int)(code & 31u);
+    if ((code >> 8) != 0) {
 #pragma unroll
-        for (int c = 0; c < 6; ++c) acc[c] += sv * d[c];
+        for (int c = 0; c < 6; ++c) G.V[c][r * (r + 1) / 2 + ix] = acc[c];
+    } else {
+        double d[6], p[6];
+        load_d6(G.D[kDOff[r] + ix], d);
+#pragma unroll
+        for (int c = 0; c < 6; ++c) p[c] = d[c] * acc[c];
+        store_d6(G.ACC[kStOff[r] + ix], p);
     }
-    store_d6(G.ACC[R], acc);
 }
 
-__device__ __forceinline__ void heavy_ghost(const Inst& I, const GhostRec& Rg, GhostWarp& G,
-                                            const double* __restrict__ rec, int lane, int stage, int row1, int row2,
-                                            unsigned vitem, const double s0[6], const double s1[6],
-                                            const double* next_rec) {
+// two rows of one order for all six fields c, each summed over b in order
+// (bc1.rs:224-236)
+__device__ __forceinline__ void dot_pair(GhostWarp& G, const double* __restrict__ rec, unsigned codes) {
+    if (codes == kPairNone) return;
+    const unsigned c1 = codes & 0xffffu, c2 = codes >> 16;
+    const int r = (int)((c1 >> 5) & 7u);
+    const int m = (r + 1) * (r + 1);
+    const double(*__restrict__ D)[6] = G.D + kDOff[r];
+    int st1, st2;
+    const double* __restrict__ p1 = row_src(rec, c1, m, st1);
+    const double* __restrict__ p2 = row_src(rec, c2, m, st2);
+    double a1[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, a2[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll 2
+    for (int b = 0; b < m; ++b) {
+        const double x1 = p1[b * st1], x2 = p2[b * st2];
+        double d[6];
+        load_d6(D[b], d);
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+            a1[c] += x1 * d[c];
+            a2[c] += x2 * d[c];
+        }
+    }
+    row_out(G, c1, a1);
+    row_out(G, c2, a2);
+}
+
+// Fetches for the warp's next ghost (record slot n_heavy, -1 for none, and
+// instance n_inst, loaded before this ghost's wait) are spread over the steps
+// so that no load waits on the one before it: its stencil indices and state
+// buffer after step 3, its stencil states (n0, n1) and its instance's error
+// flag (n_skip) after step 4, its record once step 3 has read this one.
+__device__ __forceinline__ void heavy_ghost(const Inst* __restrict__ insts, const Inst& I, const GhostRec& Rg,
+                                            GhostWarp& G, const double* __restrict__ rec,
+                                            const double* __restrict__ hrec, int lane, int stage,
+                                            unsigned slot_a, unsigned slot_b, const double s0[6],
+                                            const double s1[6], int n_heavy, int n_inst, double n0[6],
+                                            double n1[6], bool& n_skip) {
     const DevParams& P = I.P;
     double* buf = const_cast<double*>(stage_src(I, stage));
     const long long plane = I.plane;
@@ -355,38 +424,43 @@ __device__ __forceinline__ void heavy_ghost(const Inst& I, const GhostRec& Rg, G
     project_node(G, L, s0, nx, ny, lane);
     if (lane + 32 < 55) project_node(G, L, s1, nx, ny, lane + 32);
     __syncwarp();
-    // 3. rows of S_r d_c
-    acc_row(G, rec, row1);
-    if (row2 >= 0) acc_row(G, rec, row2);
+    // 3. the 70 rows: d_c,a (S_r d_c)_a and V^(k)_{c,r}
+    dot_pair(G, rec, slot_a);
+    dot_pair(G, rec, slot_b);
+    // the next ghost's stencil indices, state buffer and error flag address
+    int st0 = 0, st1 = 0;
+    const double* nbuf = nullptr;
+    long long nplane = 0;
+    const DevError* nerr = nullptr;
+    if (n_heavy >= 0) {
+        const int32_t* st = reinterpret_cast<const int32_t*>(hrec + (size_t)n_heavy * GH_REC + GH_ST);
+        st0 = __ldg(&st[lane]);
+        if (lane + 32 < 55) st1 = __ldg(&st[lane + 32]);
+        nbuf = stage_src(insts[n_inst], stage);
+        nplane = insts[n_inst].plane;
+        nerr = insts[n_inst].err;
+    }
+    double dr = 0.0;
+    if (lane < 30) dr = rec[GH_D + lane - 5 * (lane / 5)];
     __syncwarp();
-    // 4a. beta and alpha, lanes (c, r)
+    // the record is not read below: bring in the next ghost's
+    if (lane == 0 && n_heavy >= 0) bulk_load(G.rec[0], hrec + (size_t)n_heavy * GH_REC, GH_REC * 8, &G.bar[0]);
+    // 4. lanes (c, r): beta_{c,r} = sum_a d_a (S d)_a in order, alpha = d_r / (eps + beta)^q
     if (lane < 30) {
         const int c = lane / 5, r = lane - 5 * (lane / 5);
         const int m = (r + 1) * (r + 1), off = kStOff[r];
         double beta = 0.0;
-        for (int a = 0; a < m; ++a) beta += G.D[off + a][c] * G.ACC[off + a][c];
-        G.alpha[c][r] = rec[GH_D + r] / pow_q(P.eps + beta, P.weno_q);
-    }
-    // 4b. V^(k)_{c,r} = w_{r,k} . d_c for the six c of item (r, k)
-    if (vitem != 0xffu) {
-        const int r = (int)(vitem >> 3), k = (int)(vitem & 7u);
-        const int m = (r + 1) * (r + 1), off = kStOff[r];
-        const double* __restrict__ w = rec + GH_W + kWOff[r] + k * m;
-        double v[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
 #pragma unroll 5
-        for (int a = 0; a < m; ++a) {
-            const double wa = w[a];
-            double d[6];
-            load_d6(G.D[off + a], d);
-#pragma unroll
-            for (int c = 0; c < 6; ++c) v[c] += wa * d[c];
-        }
-#pragma unroll
-        for (int c = 0; c < 6; ++c) G.V[c][r * (r + 1) / 2 + k] = v[c];
+        for (int a = 0; a < m; ++a) beta += G.ACC[off + a][c];
+        G.alpha[c][r] = dr / pow_q(P.eps + beta, P.weno_q);
+    }
+    // the next ghost's stencil states (used in its step 2) and error flag
+    if (n_heavy >= 0) {
+        load6(nbuf, nplane, st0, n0);
+        if (lane + 32 < 55) load6(nbuf, nplane, st1, n1);
+        n_skip = nerr->key != ~0ull;
     }
     __syncwarp();
-    // the record is not read below: bring in the next ghost's
-    if (lane == 0 && next_rec) bulk_load(G.rec[0], next_rec, GH_REC * 8, &G.bar[0]);
     // 5. nonlinear weights (bc1.rs:247-252); V^(k)_r = 0 for k > r
     if (lane < 30) {
         const int k = lane / 6, c = lane - 6 * (lane / 6);
@@ -466,38 +540,33 @@ __global__ void __launch_bounds__(GH_WARPS * 32, GH_BLOCKS_PER_SM) k_ghosts(cons
     const int stride = gridDim.x * GH_WARPS;
     int g = blockIdx.x * GH_WARPS + (threadIdx.x >> 5);
     if (g < nh) { // warp-uniform
-        // per-lane schedules of steps 3 and 4
-        const int row1 = lane < 25 ? 30 + lane : 14 + (lane - 25);
-        const int row2 = lane < 2 ? 28 + lane
-                         : lane < 11 ? 5 + (lane - 2)
-                         : lane < 15 ? 1 + (lane - 11)
-                         : lane == 15 ? 0
-                         : lane >= 25 ? 21 + (lane - 25) : -1;
-        const unsigned vitem = kVItem[lane];
+        const unsigned slot_a = kSlotA[lane], slot_b = kSlotB[lane];
         if (lane == 0) {
             mbar_init(&G.bar[0]);
             mbar_fence_init();
             bulk_load(G.rec[0], hrec + (size_t)heavy[g].heavy * GH_REC, GH_REC * 8, &G.bar[0]);
         }
         __syncwarp();
-        // stencil states of the warp's first ghost; later ones are gathered one
-        // ghost ahead, while the current one is processed
+        // stencil states of the warp's first ghost; later ones are gathered
+        // while the ghost before them is processed
         double s0[6], s1[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        bool skip;
         {
             const GhostRec& R0 = heavy[g];
             gather_stencil(insts[R0.inst], hrec + (size_t)R0.heavy * GH_REC, lane, stage, s0, s1);
+            skip = has_error(insts[R0.inst]);
         }
         for (int it = 0; g < nh; ++it, g += stride) {
             const int gn = g + stride;
-            const double* next_rec = gn < nh ? hrec + (size_t)heavy[gn].heavy * GH_REC : nullptr;
+            int n_heavy = -1, n_inst = 0;
+            if (gn < nh) {
+                n_heavy = __ldg(&heavy[gn].heavy);
+                n_inst = __ldg(&heavy[gn].inst);
+            }
             const GhostRec Rg = heavy[g];
             const Inst& I = insts[Rg.inst];
-            const bool skip = has_error(I);
+            bool n_skip = false;
             double n0[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, n1[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-            if (gn < nh) {
-                const GhostRec& Rn = heavy[gn];
-                gather_stencil(insts[Rn.inst], hrec + (size_t)Rn.heavy * GH_REC, lane, stage, n0, n1);
-            }
             const bool ok = __all_sync(0xffffffffu, mbar_wait(&G.bar[0], (uint32_t)(it & 1)));
             if (!ok) {
                 if (lane == 0) report(I, 1 + 2 * stage, GH_TIMEOUT_CODE, (unsigned)Rg.gid);
@@ -505,9 +574,16 @@ __global__ void __launch_bounds__(GH_WARPS * 32, GH_BLOCKS_PER_SM) k_ghosts(cons
             }
             for (int e = lane; e < GH_LR; e += 32) G.LR[e] = G.rec[0][GH_L + e];
             __syncwarp();
-            if (!skip) heavy_ghost(I, Rg, G, G.rec[0], lane, stage, row1, row2, vitem, s0, s1, next_rec);
-            else if (lane == 0 && next_rec) bulk_load(G.rec[0], next_rec, GH_REC * 8, &G.bar[0]);
+            if (!skip) {
+                heavy_ghost(insts, I, Rg, G, G.rec[0], hrec, lane, stage, slot_a, slot_b, s0, s1, n_heavy,
+                            n_inst, n0, n1, n_skip);
+            } else if (n_heavy >= 0) {
+                if (lane == 0) bulk_load(G.rec[0], hrec + (size_t)n_heavy * GH_REC, GH_REC * 8, &G.bar[0]);
+                gather_stencil(insts[n_inst], hrec + (size_t)n_heavy * GH_REC, lane, stage, n0, n1);
+                n_skip = has_error(insts[n_inst]);
+            }
             __syncwarp();
+            skip = n_skip;
 #pragma unroll
             for (int q = 0; q < 6; ++q) { s0[q] = n0[q]; s1[q] = n1[q]; }
         }
