@@ -34,6 +34,7 @@
 #include "dual.cuh"
 #include "kernels.cuh"
 #include "physics.cuh"
+#include "ghost_rows.cuh"
 
 namespace rh3t {
 
@@ -311,10 +312,13 @@ __device__ __forceinline__ void r_base_vjp2(const double base[5], const DevParam
             if (DIR == 0) bv += t3;
             else bu += t3;
         } else { // species k: (1, u, v, ..., gt w2 / (6 g_k) at row 3 + k)
+            // (selects, not an index: a runtime index would put Rb2 in local memory)
             const int k = DIR == 0 ? c - 1 : c - 2;
+            const double rk = k == 0 ? r[3] : (k == 1 ? r[4] : r[5]);
+            const double gkk = k == 0 ? gk[0] : (k == 1 ? gk[1] : gk[2]);
             bu += r[1];
             bv += r[2];
-            bw2 += gt * K6 / gk[k] * r[3 + k];
+            bw2 += gt * K6 / gkk * rk;
         }
         bvel += lamb2[h];
     }
@@ -589,10 +593,15 @@ __device__ void adj_flux_tile(const Inst& I, const Tile& t, const double* __rest
         }
         __syncthreads(); // LB, WB, FK, G and LAMB are read: reuse them
         if (on) {
-            if (part == 0) for (int m = 0; m < 5; ++m) S.FK[0][m][f] = bb[m];
-            if (part == 1) for (int m = 0; m < 5; ++m) S.G[m][f] = bb[m];
-            if (part == 2) for (int m = 0; m < 5; ++m) S.LAMB[m][f] = bb[m];
+#pragma unroll
+            for (int m = 0; m < 5; ++m) {
+                if (part == 0) S.FK[0][m][f] = bb[m];
+                if (part == 1) S.G[m][f] = bb[m];
+                if (part == 2) S.LAMB[m][f] = bb[m];
+            }
+#pragma unroll
             for (int h = 0; h < 2; ++h)
+#pragma unroll
                 for (int m = 0; m < 6; ++m) {
                     S.LB[2 * part + h][m][f] = V[h][m];
                     S.WB[2 * part + h][m][f] = VF[h][m];
@@ -600,6 +609,7 @@ __device__ void adj_flux_tile(const Inst& I, const Tile& t, const double* __rest
         }
         __syncthreads();
         if (on && part < 2) { // the Roe average's vjp: point 3 on part 0, point 2 on part 1
+#pragma unroll
             for (int m = 0; m < 5; ++m) bb[m] = S.FK[0][m][f] + (S.G[m][f] + S.LAMB[m][f]);
             int i, j, p0, ps;
             adj_face_index<DIR>(t, f, i, j, p0, ps);
@@ -620,6 +630,7 @@ __device__ void adj_flux_tile(const Inst& I, const Tile& t, const double* __rest
                 const double Db[3] = {S.FB[3][f] / sc * cx, S.FB[4][f] / sc * cx, S.FB[5][f] / sc * cx};
                 const double cf[6] = {-2.0, 25.0, -245.0, 245.0, -25.0, 2.0};
                 const double kap[3] = {P.kappa_e, P.kappa_i, P.kappa_r};
+#pragma unroll
                 for (int k = 0; k < 6; ++k) {
                     double uk[6];
                     adj_point(S, p0 + k * ps, uk, F_);
@@ -655,6 +666,7 @@ __device__ void adj_flux_tile(const Inst& I, const Tile& t, const double* __rest
             }
             if (!S.act[f]) continue;
             any = true;
+#pragma unroll
             for (int m = 0; m < 6; ++m) {
                 ub[m] += S.LB[k][m][f]; // V_k of face f
                 fb[m] += S.WB[k][m][f]; // VF_k
@@ -897,23 +909,12 @@ __constant__ int kAStOff[6] = {0, 1, 5, 14, 30, 55};
 __constant__ int kASOff[6] = {0, 1, 17, 98, 354, 979};
 __constant__ int kAWOff[6] = {0, 1, 9, 36, 100, 225};
 
-// the 90 dot products V^(k)_{c,r} = w_{r,k} . d_c as (c << 6) | (r << 3) | k,
-// longest first: lane l takes entries l, l + 32, l + 64
-__constant__ unsigned short kAdjVItems[90] = {
-    0x020, 0x021, 0x022, 0x023, 0x024, 0x060, 0x061, 0x062, 0x063, 0x064,
-    0x0a0, 0x0a1, 0x0a2, 0x0a3, 0x0a4, 0x0e0, 0x0e1, 0x0e2, 0x0e3, 0x0e4,
-    0x120, 0x121, 0x122, 0x123, 0x124, 0x160, 0x161, 0x162, 0x163, 0x164,
-    0x018, 0x019, 0x01a, 0x01b, 0x058, 0x059, 0x05a, 0x05b, 0x098, 0x099,
-    0x09a, 0x09b, 0x0d8, 0x0d9, 0x0da, 0x0db, 0x118, 0x119, 0x11a, 0x11b,
-    0x158, 0x159, 0x15a, 0x15b, 0x010, 0x011, 0x012, 0x050, 0x051, 0x052,
-    0x090, 0x091, 0x092, 0x0d0, 0x0d1, 0x0d2, 0x110, 0x111, 0x112, 0x150,
-    0x151, 0x152, 0x008, 0x009, 0x048, 0x049, 0x088, 0x089, 0x0c8, 0x0c9,
-    0x108, 0x109, 0x148, 0x149, 0x000, 0x040, 0x080, 0x0c0, 0x100, 0x140};
 
 struct AdjGhostWarp {
     double L[36], R[36], lam[6];             // L[6c + j]; R column c at R[6c + i]
     double U6[6][56];                        // rotated stencil states
-    double D[6][56], ACC[6][56], STD[6][56]; // STD: D-bar
+    double D[56][6];                         // d_c of stencil node a at row d_row(a)
+    double ACC[6][56], STD[6][56];           // ACC: S d; STD: D-bar
     double alpha[6][5], beta[6][5], V[6][5][5];
     double v[5][6], x[5][6], ub[5][6], xb[5][6], vinf[6], vinfb[6];
     double Lb[6][6], Rb[6][6];
@@ -1129,6 +1130,62 @@ __device__ __noinline__ bool wall_outflow_vjp(const Inst& I, const GhostRec& Rg,
     return true;
 }
 
+// two rows of one order of the record (S_r transposed, stride m, or w_{r,k},
+// stride 1; read from global memory, prefetched to L2) with the stencil
+// data d, all six fields: an S row stores (S_r d_c)_a, a w row V^(k)_{c,r}
+__device__ __forceinline__ void adj_dot_pair(AdjGhostWarp& G, const double* __restrict__ rec, unsigned codes) {
+    if (codes == kPairNone) return;
+    const unsigned c1 = codes & 0xffffu, c2 = codes >> 16;
+    const int r = (int)((c1 >> 5) & 7u), m = (r + 1) * (r + 1);
+    const int i1 = (int)(c1 & 31u), i2 = (int)(c2 & 31u);
+    const bool w1 = (c1 >> 8) != 0, w2 = (c2 >> 8) != 0;
+    const double* __restrict__ p1 = w1 ? rec + GH_W + kAWOff[r] + i1 * m : rec + GH_S + kASOff[r] + i1;
+    const double* __restrict__ p2 = w2 ? rec + GH_W + kAWOff[r] + i2 * m : rec + GH_S + kASOff[r] + i2;
+    const int s1 = w1 ? 1 : m, s2 = w2 ? 1 : m;
+    const double(*__restrict__ D)[6] = G.D + kDOff[r];
+    double a1[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, a2[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    // the record is read from L2: the loads of the next four terms are in
+    // flight while four terms are summed (in order)
+    constexpr int PF = 4;
+    double x1[PF], x2[PF];
+#pragma unroll
+    for (int j = 0; j < PF; ++j) {
+        x1[j] = j < m ? __ldg(p1 + j * s1) : 0.0;
+        x2[j] = j < m ? __ldg(p2 + j * s2) : 0.0;
+    }
+    for (int b0 = 0; b0 < m; b0 += PF) {
+        double y1[PF], y2[PF];
+#pragma unroll
+        for (int j = 0; j < PF; ++j) {
+            const int bn = b0 + PF + j;
+            y1[j] = bn < m ? __ldg(p1 + bn * s1) : 0.0;
+            y2[j] = bn < m ? __ldg(p2 + bn * s2) : 0.0;
+        }
+#pragma unroll
+        for (int j = 0; j < PF; ++j) {
+            if (b0 + j < m) {
+                double d[6];
+                load_d6(D[b0 + j], d);
+#pragma unroll
+                for (int c = 0; c < 6; ++c) {
+                    a1[c] += x1[j] * d[c];
+                    a2[c] += x2[j] * d[c];
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < PF; ++j) { x1[j] = y1[j]; x2[j] = y2[j]; }
+    }
+    const int off = kAStOff[r];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+        if (w1) G.V[c][r][i1] = a1[c];
+        else G.ACC[c][off + i1] = a1[c];
+        if (w2) G.V[c][r][i2] = a2[c];
+        else G.ACC[c][off + i2] = a2[c];
+    }
+}
+
 // L2 prefetch of a ghost's record by the bulk-copy engine (16-byte aligned,
 // size a multiple of 16; nothing waits on it)
 __device__ __forceinline__ void prefetch_record_l2(const double* rec) {
@@ -1147,52 +1204,52 @@ __device__ void ghost_vjp_warp(const Inst& I, const GhostRec& Rg, const double* 
     const double nx = Rg.nx, ny = Rg.ny;
     // the record's S_r and w are read in steps below: have them in L2 first
     if (lane == 0) prefetch_record_l2(rec);
-    // L, R, lambda at the nearest node of X (k_adj_ghost_lr)
-    for (int e = lane; e < 78; e += 32) {
-        const double v = slot[e];
-        if (e < 36) G.L[e] = v;
-        else if (e < 72) G.R[e - 36] = v;
-        else G.lam[e - 72] = v;
+    // L, R, lambda at the nearest node of X (k_adj_ghost_lr), the stencil
+    // indices and then the stencil states: all loads in flight together
+    double sl[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) sl[j] = lane + 32 * j < 78 ? slot[lane + 32 * j] : 0.0;
+    const int32_t* st = reinterpret_cast<const int32_t*>(rec + GH_ST);
+    const int i0 = __ldg(&st[lane]), i1 = lane + 32 < 55 ? __ldg(&st[lane + 32]) : 0;
+    double sx0[6], sx1[6];
+    load6(X, plane, i0, sx0);
+    if (lane + 32 < 55) load6(X, plane, i1, sx1);
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        const int e = lane + 32 * j;
+        if (e < 36) G.L[e] = sl[j];
+        else if (e < 72) G.R[e - 36] = sl[j];
+        else if (e < 78) G.lam[e - 72] = sl[j];
     }
     __syncwarp();
     const double* L = G.L;    // L[c][j] = L[6c + j]
     const double* Rc = G.R;   // R[i][c] = Rc[6c + i]
     const double* lam = G.lam;
-    const int32_t* st = reinterpret_cast<const int32_t*>(rec + GH_ST);
-    const double* S = rec + GH_S;   // transposed per order: S_r[a][b] = S[off + b m + a]
     // ---- forward: D, ACC = S d, beta, alpha, V, v. S_r = P^T M_r P is
     // symmetric (bc1.rs:169-175), so d beta / d d = 2 S d: S^T d is not formed
-    for (int a = lane; a < 55; a += 32) {
-        double s[6];
-        load6(X, plane, st[a], s);
+    auto project = [&](int a, const double s[6]) {
         const double u6[6] = {s[0], s[1] * nx + s[2] * ny, -s[1] * ny + s[2] * nx, s[3], s[4], s[5]};
         for (int q = 0; q < 6; ++q) G.U6[q][a] = u6[q];
+        double d[6];
         for (int c = 0; c < 6; ++c) {
             double acc = 0.0;
             for (int q = 0; q < 6; ++q) acc += L[6 * c + q] * u6[q];
-            G.D[c][a] = acc;
+            d[c] = acc;
         }
-    }
+        store_d6(G.D[d_row(a)], d);
+    };
+    project(lane, sx0);
+    if (lane + 32 < 55) project(lane + 32, sx1);
     __syncwarp();
-    for (int a = lane; a < 55; a += 32) {
-        const int r = aorder(a), m = (r + 1) * (r + 1), off = kAStOff[r], ar = a - off;
-        const double* Sr = S + kASOff[r];
-        double acc[6] = {0, 0, 0, 0, 0, 0};
-#pragma unroll 5
-        for (int b = 0; b < m; ++b) {
-            const double sab = Sr[b * m + ar]; // S[a][b]
-#pragma unroll
-            for (int c = 0; c < 6; ++c) acc[c] += sab * G.D[c][off + b]; // (S d)_a
-        }
-#pragma unroll
-        for (int c = 0; c < 6; ++c) G.ACC[c][a] = acc[c];
-    }
+    // the 70 rows (S d)_a and V^(k)_{c,r} = w_{r,k} . d_c, as pairs of rows of one order
+    adj_dot_pair(G, rec, kSlotA[lane]);
+    adj_dot_pair(G, rec, kSlotB[lane]);
     __syncwarp();
     if (lane < 30) {
         const int c = lane / 5, r = lane - 5 * (lane / 5);
-        const int m = (r + 1) * (r + 1), off = kAStOff[r];
+        const int m = (r + 1) * (r + 1), off = kAStOff[r], doff = kDOff[r];
         double beta = 0.0;
-        for (int a = 0; a < m; ++a) beta += G.D[c][off + a] * G.ACC[c][off + a];
+        for (int a = 0; a < m; ++a) beta += G.D[doff + a][c] * G.ACC[c][off + a];
         G.beta[c][r] = beta;
         const double x = P.eps + beta;
         double xq;
@@ -1200,15 +1257,6 @@ __device__ void ghost_vjp_warp(const Inst& I, const GhostRec& Rg, const double* 
         else xq = pow(x, P.weno_q);
         G.alpha[c][r] = rec[GH_D + r] / xq;
         for (int k = r + 1; k < 5; ++k) G.V[c][r][k] = 0.0;
-    }
-    for (int q = lane; q < 90; q += 32) {
-        const unsigned e = kAdjVItems[q];
-        const int c = (int)(e >> 6), r = (int)((e >> 3) & 7u), k = (int)(e & 7u);
-        const int m = (r + 1) * (r + 1), off = kAStOff[r];
-        const double* w = rec + GH_W + kAWOff[r] + k * m;
-        double v = 0.0;
-        for (int a = 0; a < m; ++a) v += w[a] * G.D[c][off + a];
-        G.V[c][r][k] = v;
     }
     __syncwarp();
     if (lane < 30) {
@@ -1312,22 +1360,44 @@ __device__ void ghost_vjp_warp(const Inst& I, const GhostRec& Rg, const double* 
         for (int k = 0; k < 5; ++k) G.V[oc][orr][k] = om * G.vb[k][oc];                 // now V-bar
     }
     __syncwarp();
-    // D-bar over the 55 nodes: beta = d^T S d, V = w . d
-    for (int a = lane; a < 55; a += 32) {
-        const int r = aorder(a), m = (r + 1) * (r + 1), off = kAStOff[r], ar = a - off;
+    // D-bar over the 55 nodes: beta = d^T S d, V = w . d (the w columns of
+    // both of a lane's nodes are loaded together)
+    {
+        const int r0 = aorder(lane), m0 = (r0 + 1) * (r0 + 1), ar0 = lane - kAStOff[r0];
+        const int ar1 = lane + 32 - kAStOff[4]; // the second node is of order 4
+        double wv0[5], wv1[5];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+            wv0[k] = k <= r0 ? __ldg(&rec[GH_W + kAWOff[r0] + k * m0 + ar0]) : 0.0;
+            wv1[k] = lane + 32 < 55 ? __ldg(&rec[GH_W + kAWOff[4] + k * 25 + ar1]) : 0.0;
+        }
         for (int c = 0; c < 6; ++c) {
-            double acc = G.beta[c][r] * (2.0 * G.ACC[c][a]);
-            for (int k = 0; k <= r; ++k) acc += G.V[c][r][k] * rec[GH_W + kAWOff[r] + k * m + ar];
-            G.STD[c][a] = acc; // D-bar
+            double acc = G.beta[c][r0] * (2.0 * G.ACC[c][lane]);
+            for (int k = 0; k <= r0; ++k) acc += G.V[c][r0][k] * wv0[k];
+            G.STD[c][lane] = acc; // D-bar
+        }
+        if (lane + 32 < 55) {
+            for (int c = 0; c < 6; ++c) {
+                double acc = G.beta[c][4] * (2.0 * G.ACC[c][lane + 32]);
+#pragma unroll
+                for (int k = 0; k < 5; ++k) acc += G.V[c][4][k] * wv1[k];
+                G.STD[c][lane + 32] = acc;
+            }
         }
     }
     __syncwarp();
-    // D = L rot(u_a): Lb += DB rot(u_a)^T, rot(u_a)-bar = L^T DB
-    for (int e = lane; e < 36; e += 32) {
-        const int c = e / 6, q = e - 6 * (e / 6);
-        double acc = 0.0;
-        for (int a = 0; a < 55; ++a) acc += G.STD[c][a] * G.U6[q][a];
-        G.Lb[c][q] += acc;
+    // D = L rot(u_a): Lb += DB rot(u_a)^T (18 lanes, entries (c, q) and (c, q + 1)),
+    // rot(u_a)-bar = L^T DB
+    if (lane < 18) {
+        const int c = lane / 3, q = 2 * (lane - 3 * (lane / 3));
+        double acc0 = 0.0, acc1 = 0.0;
+        for (int a = 0; a < 55; ++a) {
+            const double sd = G.STD[c][a];
+            acc0 += sd * G.U6[q][a];
+            acc1 += sd * G.U6[q + 1][a];
+        }
+        G.Lb[c][q] += acc0;
+        G.Lb[c][q + 1] += acc1;
     }
     for (int a = lane; a < 55; a += 32) {
         double ur[6];
@@ -1337,7 +1407,7 @@ __device__ void ghost_vjp_warp(const Inst& I, const GhostRec& Rg, const double* 
             ur[q] = acc;
         }
         const double sb[6] = {ur[0], ur[1] * nx - ur[2] * ny, ur[1] * ny + ur[2] * nx, ur[3], ur[4], ur[5]};
-        atomic_add6(Ub, plane, st[a], sb);
+        atomic_add6(Ub, plane, a == lane ? i0 : i1, sb);
     }
     __syncwarp();
     // L, R of the nearest node: L-bar folded into R-bar (lanes over the 36

@@ -208,7 +208,8 @@ __device__ __forceinline__ void flux_tile(const Inst& I, const Tile& t, int stag
     }
 }
 
-__global__ void __launch_bounds__(FLUX_THREADS) k_flux(const Inst* __restrict__ insts, const Tile* __restrict__ tx,
+// 64 registers: 5 blocks (30 warps) per SM instead of 4 at the uncapped 76
+__global__ void __launch_bounds__(FLUX_THREADS, 5) k_flux(const Inst* __restrict__ insts, const Tile* __restrict__ tx,
                                                        int ntx, const Tile* __restrict__ ty, int nty, int stage) {
     __shared__ FluxShared S;
     const int b = blockIdx.x;
