@@ -1209,6 +1209,10 @@ __device__ void ghost_vjp_warp(const Inst& I, const GhostRec& Rg, const double* 
     double sl[3];
 #pragma unroll
     for (int j = 0; j < 3; ++j) sl[j] = lane + 32 * j < 78 ? slot[lane + 32 * j] : 0.0;
+    // read much later, loaded now: the cotangent at the ghost node and the
+    // FarField state, component `lane` on lanes 0-5
+    const double w_gn = lane < 6 ? W[lane * plane + Rg.node] : 0.0;
+    const double ui_l = lane < 6 ? I.bcs[Rg.bc].state[lane] : 0.0;
     const int32_t* st = reinterpret_cast<const int32_t*>(rec + GH_ST);
     const int i0 = __ldg(&st[lane]), i1 = lane + 32 < 55 ? __ldg(&st[lane + 32]) : 0;
     double sx0[6], sx1[6];
@@ -1268,8 +1272,9 @@ __device__ void ghost_vjp_warp(const Inst& I, const GhostRec& Rg, const double* 
         G.v[k][c] = res;
     }
     __syncwarp();
-    const DevBC& bc = I.bcs[Rg.bc];
-    const double* ui = bc.state;
+    double ui[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) ui[q] = __shfl_sync(0xffffffffu, ui_l, q);
     const double uinf[6] = {ui[0], ui[1] * nx + ui[2] * ny, -ui[1] * ny + ui[2] * nx, ui[3], ui[4], ui[5]};
     if (lane < 6) {
         double acc = 0.0;
@@ -1282,10 +1287,10 @@ __device__ void ghost_vjp_warp(const Inst& I, const GhostRec& Rg, const double* 
         G.x[k][m2] = lam[m2] < 0.0 ? (k == 0 ? G.vinf[m2] : 0.0) : G.v[k][m2];
     }
     // ---- reverse: rotation back and Taylor sum
-    const long long gn = Rg.node;
+    double o[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) o[q] = __shfl_sync(0xffffffffu, w_gn, q);
     if (lane == 0) {
-        const double o[6] = {W[gn], W[plane + gn], W[2 * plane + gn], W[3 * plane + gn], W[4 * plane + gn],
-                             W[5 * plane + gn]};
         // out1 = mn nx - mt ny, out2 = mn ny + mt nx
         const double gb[6] = {o[0], o[1] * nx + o[2] * ny, -o[1] * ny + o[2] * nx, o[3], o[4], o[5]};
         double coef = 1.0;
