@@ -54,8 +54,8 @@ FLUX_TRAFFIC_BYTES = {"cyl961": 651.5e6}
 # k_ghosts) and per active face of one k_flux launch, from ncu captures on
 # the batch24 workload (84,000 heavy ghosts, 1,714,456 faces), scaled by the
 # heavy-ghost and face counts of the batched workloads
-GHOST_TRAFFIC_PER_HEAVY = (902.84e6 + 7.47e6 + 15.32e6 + 9.71e6) / 84000
-FLUX_TRAFFIC_PER_FACE = (77.82e6 + 42.39e6) / 1714456
+GHOST_TRAFFIC_PER_HEAVY = (902.88e6 + 7.24e6 + 15.32e6 + 9.25e6) / 84000
+FLUX_TRAFFIC_PER_FACE = (74.60e6 + 43.63e6) / 1714456
 FALLBACK_HBM_GBS = 6650.0
 
 
