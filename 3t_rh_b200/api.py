@@ -574,6 +574,19 @@ class Batch(_SnapshotIO):
         t = _arr(times, np.float64)
         self._check(self.L.rh3t_upload_batch(self.h, v.ctypes.data, t.ctypes.data))
 
+    def step_host(self, values, times, cfl_factor=0.05, groups=8):
+        """One time-loop iteration of every instance on host arrays, in place
+        (values: total_cells x 6, times: n; float64, C-contiguous; page-locked
+        memory lets the copies of one instance group overlap the step of
+        another)."""
+        if values.dtype != np.float64 or not values.flags.c_contiguous or values.size != int(self.offsets[-1]) * 6:
+            raise ValueError("values must be a C-contiguous float64 array of total_cells x 6")
+        if times.dtype != np.float64 or not times.flags.c_contiguous or times.size != self.n:
+            raise ValueError("times must be a C-contiguous float64 array of n instances")
+        self._check(self.L.rh3t_step_host_batch(self.h, values.ctypes.data, times.ctypes.data, float(cfl_factor),
+                                                int(groups)))
+        return values, times
+
     def download_values(self, out=None, times=None):
         """(total_cells x 6 values of all instances, times[n]); out / times
         (float64, C-contiguous, e.g. pinned host memory) receive the copy

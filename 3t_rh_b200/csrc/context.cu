@@ -728,6 +728,9 @@ extern "C" void rh3t_destroy(rh3t_ctx* c) {
     io_free(c);
     adj_free(c);
     if (c->graph) cudaGraphExecDestroy(c->graph);
+    for (cudaStream_t x : c->xfer)
+        if (x) cudaStreamDestroy(x);
+    if (c->h_sc) cudaFreeHost(c->h_sc);
     dfree(c->d_state); dfree(c->d_mask); dfree(c->d_faces); dfree(c->d_bcs); dfree(c->d_sc); dfree(c->d_err);
     dfree(c->d_times); dfree(c->d_inst); dfree(c->d_ghosts); dfree(c->d_gpart); dfree(c->d_hrec);
     dfree(c->d_tx); dfree(c->d_ty); dfree(c->d_tc); dfree(c->d_tr); dfree(c->d_io); dfree(c->d_io2);
@@ -859,6 +862,89 @@ extern "C" int rh3t_step_host(rh3t_ctx* c, double* value, double* time, double c
                               cudaMemcpyDeviceToHost, s));
     CK(c, cudaGetLastError());
     return fetch_error(c, all(c));
+}
+
+// Host value arrays in, one step, host value arrays out, with the copies of
+// one group of instances overlapping the step of another: instance groups of
+// about equal cell counts go host -> device on one copy stream, take their
+// step on the context's stream (eager launches over the group's instance
+// range) and return on a second copy stream.
+extern "C" int rh3t_step_host_batch(rh3t_ctx* c, double* values, double* times, double cfl_factor,
+                                    int32_t n_groups) {
+    if (!c || !values || !times) return RH3T_ERR_INVALID_ARGUMENT;
+    CK(c, cudaSetDevice(c->device));
+    for (cudaStream_t& x : c->xfer)
+        if (!x) CK(c, cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
+    if (!c->h_sc) CK(c, cudaMallocHost((void**)&c->h_sc, (size_t)c->n_inst * sizeof(DevScalars)));
+    const int groups = std::max(1, std::min(n_groups > 0 ? n_groups : 8, c->n_inst));
+    std::vector<Span> gr;
+    {
+        const long long total = c->total_cells;
+        int k0 = 0;
+        for (int g = 0; g < groups && k0 < c->n_inst; ++g) {
+            const long long target = total * (g + 1) / groups;
+            int k1 = k0 + 1;
+            while (k1 < c->n_inst && c->hi[k1].cell_off + c->hi[k1].nx * c->hi[k1].ny <= target) ++k1;
+            if (g == groups - 1) k1 = c->n_inst;
+            gr.push_back(Span{k0, k1});
+            k0 = k1;
+        }
+        if (k0 < c->n_inst) gr.back().k1 = c->n_inst;
+    }
+    const int G = (int)gr.size();
+    cudaStream_t sc = c->stream, su = c->xfer[0], sd = c->xfer[1];
+    int rc = set_step_params(c, cfl_factor, INFINITY, all(c));
+    if (rc) return rc;
+    std::vector<cudaEvent_t> ev((size_t)(2 * G + 2), nullptr);
+    auto release = [&]() {
+        for (cudaEvent_t e : ev)
+            if (e) cudaEventDestroy(e);
+    };
+    for (cudaEvent_t& e : ev) {
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+            release();
+            return set_error(c, RH3T_ERR_CUDA, "event create failed");
+        }
+    }
+    auto ck = [&](cudaError_t e, const char* where) {
+        if (e == cudaSuccess) return 0;
+        release();
+        return cuda_check(c, e, where);
+    };
+#define CKE(call) do { if (int _rc = ck((call), #call)) return _rc; } while (0)
+    CKE(cudaEventRecord(ev[0], sc)); // the step parameters are set
+    CKE(cudaStreamWaitEvent(su, ev[0], 0));
+    CKE(cudaMemcpyAsync(c->d_times, times, (size_t)c->n_inst * sizeof(double), cudaMemcpyHostToDevice, su));
+    for (int g = 0; g < G; ++g) {
+        long long maxc = 0;
+        const long long cells = range_cells(c, gr[g], &maxc);
+        const long long o = 6 * c->hi[gr[g].k0].cell_off;
+        CKE(cudaMemcpyAsync(c->d_io + o, values + o, (size_t)cells * 6 * sizeof(double), cudaMemcpyHostToDevice, su));
+        launch_scatter(su, c->d_inst, gr[g].k0, gr[g].k1 - gr[g].k0, maxc, c->d_io, c->d_times);
+        CKE(cudaEventRecord(ev[1 + g], su));
+    }
+    for (int g = 0; g < G; ++g) {
+        long long maxc = 0;
+        const long long cells = range_cells(c, gr[g], &maxc);
+        const long long o = 6 * c->hi[gr[g].k0].cell_off;
+        CKE(cudaStreamWaitEvent(sc, ev[1 + g], 0));
+        enqueue_step(c, gr[g]);
+        CKE(cudaEventRecord(ev[1 + G + g], sc));
+        CKE(cudaStreamWaitEvent(sd, ev[1 + G + g], 0));
+        launch_gather(sd, c->d_inst, gr[g].k0, gr[g].k1 - gr[g].k0, maxc, c->d_io);
+        CKE(cudaMemcpyAsync(values + o, c->d_io + o, (size_t)cells * 6 * sizeof(double), cudaMemcpyDeviceToHost, sd));
+        CKE(cudaMemcpyAsync(c->h_sc + gr[g].k0, c->d_sc + gr[g].k0, (size_t)(gr[g].k1 - gr[g].k0) * sizeof(DevScalars),
+                            cudaMemcpyDeviceToHost, sd));
+    }
+    CKE(cudaEventRecord(ev[1 + 2 * G], sd));
+    CKE(cudaStreamWaitEvent(sc, ev[1 + 2 * G], 0));
+    c->launches += 2 * G;
+    CKE(cudaGetLastError());
+#undef CKE
+    rc = fetch_error(c, all(c)); // synchronises the context's stream, and so both copy streams
+    release();
+    for (int k = 0; k < c->n_inst; ++k) times[k] = c->h_sc[k].t_after;
+    return rc;
 }
 
 extern "C" int rh3t_profile_steps(rh3t_ctx* c, int32_t nsteps, double cfl_factor, double* ms_out,

@@ -68,6 +68,8 @@ struct rh3t_ctx {
     struct rh3t_io* io = nullptr; // snapshot and diagnostic buffers (io.cu)
     int n_ghosts = 0, n_heavy = 0, n_gheavy = 0, n_gcheap = 0, max_ghosts = 0;
     cudaGraphExec_t graph = nullptr;
+    cudaStream_t xfer[2] = {nullptr, nullptr};  // host-copy streams of rh3t_step_host_batch (in, out)
+    rh3t::DevScalars* h_sc = nullptr;            // pinned: the instances' scalars read back by it
     long long launches = 0;
     rh3t_error last{};
     std::vector<int32_t> inst_status;

@@ -418,18 +418,20 @@ def run_batch(args, rh, flops, torch, dist, world, rank, local):
         vals, times = b.download_values()
         host = torch.empty(vals.shape, dtype=torch.float64, pin_memory=True).numpy()
         host[:] = vals
+        times = np.ascontiguousarray(times)
         k_e2e = max(3, min(args.steps, 10))
+        b.step_host(host, times, CFL, groups=args.e2e_groups)  # first call: its streams and buffer
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(k_e2e):
-            b.upload_values(host, times)
-            b.advance(1, CFL)
-            b.download_values(out=host, times=times)
+            b.step_host(host, times, CFL, groups=args.e2e_groups)
         el = time.perf_counter() - t0
         nb = host.size * 8
         e2e = {"value": world * cells * k_e2e / el, "unit": "cell-updates/s", "h2d_bytes_per_step": nb + 8 * b.n,
-               "d2h_bytes_per_step": nb + 8 * b.n,
-               "call": "rh3t_upload_batch + rh3t_advance(1 step) + rh3t_download_batch (all Field::value arrays)",
+               "d2h_bytes_per_step": nb + 128 * b.n,
+               "call": "rh3t_step_host_batch (every step: all Field::value arrays host -> device, one step, "
+                       f"values and times device -> host; {args.e2e_groups} instance groups, the copies of one "
+                       "overlapping the step of another; pinned host arrays; wall clock)",
                "steps": k_e2e}
 
     adj = None
@@ -486,6 +488,7 @@ def main():
     ap.add_argument("--exact", action="store_true", help="bench the no-FMA-contraction build")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-groups", type=int, default=8, help="instance groups of the pipelined host step")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the one-instance-at-a-time comparison")
     ap.add_argument("--adjoint-steps", type=int, default=200)

@@ -209,6 +209,16 @@ int32_t rh3t_instance_count(const rh3t_ctx* ctx);
 int rh3t_upload_batch(rh3t_ctx* ctx, const double* values, const double* times);
 int rh3t_download_batch(rh3t_ctx* ctx, double* values, double* times);
 int rh3t_upload_instance(rh3t_ctx* ctx, int32_t k, const double* value, double time);
+/* One time-loop iteration of every instance on host arrays (main.rs:460-466
+ * for a batch): values / times as for rh3t_upload_batch, replaced by the
+ * values and times after one step of dt = cfl_factor * dt_cfl per instance.
+ * The instances are taken in n_groups groups of about equal cell counts
+ * (n_groups <= 0: 8): the host -> device copy of one group, the step of
+ * another and the device -> host copy of a third run at the same time. The
+ * overlap needs page-locked host arrays (cudaHostAlloc or a pinned tensor);
+ * with pageable ones the result is the same and the copies do not overlap.
+ * The first call allocates two streams and a small page-locked buffer. */
+int rh3t_step_host_batch(rh3t_ctx* ctx, double* values, double* times, double cfl_factor, int32_t n_groups);
 int rh3t_download_instance(rh3t_ctx* ctx, int32_t k, double* value, double* time);
 /* rh3t_l of instance k */
 int rh3t_l_instance(rh3t_ctx* ctx, int32_t k, double* rhs, double* ghost_values);

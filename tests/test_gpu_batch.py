@@ -162,3 +162,44 @@ def test_failing_instance_isolated(rh):
     for q in (0, 2):
         u, t, _ = _alone(rh, fields[q], grids[q], 4)
         assert np.array_equal(res[q][0], u) and res[q][1] == t
+
+
+@pytest.mark.parametrize("groups", [1, 2, 0, 5])
+def test_step_host_batch_matches_upload_step_download(rh, groups):
+    """rh3t_step_host_batch (copies of one instance group overlapping the
+    step of another) gives, bit for bit, upload + one step + download."""
+    import torch
+    fields = _mixed_fields(rh)
+    grids = [rh.GhostGrid.build(f) for f in fields]
+    ref = rh.Batch(fields, grids)
+    v_ref, t_ref = ref.download_values()
+    for _ in range(3):
+        ref.upload_values(v_ref, t_ref)
+        ref.advance(1, 0.05)
+        v_ref, t_ref = ref.download_values(out=v_ref, times=t_ref)
+    b = rh.Batch(fields, grids)
+    v0, t0 = b.download_values()
+    v = torch.empty(v0.shape, dtype=torch.float64, pin_memory=True).numpy()
+    v[:] = v0
+    t = t0.copy()
+    for _ in range(3):
+        b.step_host(v, t, 0.05, groups=groups)
+    assert np.array_equal(v, v_ref) and np.array_equal(t, t_ref)
+    b.close()
+    ref.close()
+
+
+def test_step_host_batch_failing_instance(rh):
+    fields = _mixed_fields(rh)[:3]
+    grids = [rh.GhostGrid.build(f) for f in fields]
+    b = rh.Batch(fields, grids)
+    v, t = b.download_values()
+    k = int(b.offsets[1]) + int(np.flatnonzero(fields[1].fluid)[150])
+    v[k, 0] = -1.0  # negative density in instance 1, injected on the host
+    with pytest.raises(rh.RH3TError) as ei:
+        for _ in range(3):
+            b.step_host(v, t, 0.05, groups=3)
+    assert ei.value.instance == 1
+    st = b.status()
+    assert st[1] != 0 and st[0] == 0 and st[2] == 0
+    b.close()
