@@ -1253,6 +1253,7 @@ __device__ void ghost_vjp_warp(const Inst& I, const GhostRec& Rg, const double* 
         const int c = lane / 5, r = lane - 5 * (lane / 5);
         const int m = (r + 1) * (r + 1), off = kAStOff[r], doff = kDOff[r];
         double beta = 0.0;
+#pragma unroll 5
         for (int a = 0; a < m; ++a) beta += G.D[doff + a][c] * G.ACC[c][off + a];
         G.beta[c][r] = beta;
         const double x = P.eps + beta;
@@ -1404,15 +1405,27 @@ __device__ void ghost_vjp_warp(const Inst& I, const GhostRec& Rg, const double* 
         G.Lb[c][q] += acc0;
         G.Lb[c][q + 1] += acc1;
     }
-    for (int a = lane; a < 55; a += 32) {
-        double ur[6];
-        for (int q = 0; q < 6; ++q) {
-            double acc = 0.0;
-            for (int c = 0; c < 6; ++c) acc += L[6 * c + q] * G.STD[c][a];
-            ur[q] = acc;
+    {
+        // both of a lane's nodes per row of L (one read of L)
+        const bool two = lane + 32 < 55;
+        double ur0[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, ur1[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+            const double d0 = G.STD[c][lane], d1 = two ? G.STD[c][lane + 32] : 0.0;
+#pragma unroll
+            for (int q = 0; q < 6; ++q) {
+                const double l = L[6 * c + q];
+                ur0[q] += l * d0;
+                ur1[q] += l * d1;
+            }
         }
-        const double sb[6] = {ur[0], ur[1] * nx - ur[2] * ny, ur[1] * ny + ur[2] * nx, ur[3], ur[4], ur[5]};
-        atomic_add6(Ub, plane, a == lane ? i0 : i1, sb);
+        const double sb0[6] = {ur0[0], ur0[1] * nx - ur0[2] * ny, ur0[1] * ny + ur0[2] * nx, ur0[3], ur0[4], ur0[5]};
+        atomic_add6(Ub, plane, i0, sb0);
+        if (two) {
+            const double sb1[6] = {ur1[0], ur1[1] * nx - ur1[2] * ny, ur1[1] * ny + ur1[2] * nx, ur1[3], ur1[4],
+                                   ur1[5]};
+            atomic_add6(Ub, plane, i1, sb1);
+        }
     }
     __syncwarp();
     // L, R of the nearest node: L-bar folded into R-bar (lanes over the 36
