@@ -24,7 +24,8 @@ EXPORTS = (
     "rh3t_destroy", "rh3t_batch_create", "rh3t_instance_count", "rh3t_upload_batch", "rh3t_download_batch",
     "rh3t_upload_instance", "rh3t_download_instance", "rh3t_l_instance", "rh3t_calc_global_dt_batch",
     "rh3t_instance_times", "rh3t_instance_status", "rh3t_set_tile_shapes", "rh3t_get_tile_shapes",
-    "rh3t_autotune", "rh3t_l_vjp", "rh3t_adjoint_forward", "rh3t_adjoint_backward", "rh3t_snapshot",
+    "rh3t_autotune", "rh3t_l_vjp", "rh3t_adjoint_forward", "rh3t_adjoint_backward", "rh3t_adjoint_records",
+    "rh3t_adjoint_max_records", "rh3t_snapshot",
     "rh3t_snapshot_wait", "rh3t_restart", "rh3t_energy_split",
 )
 
@@ -141,6 +142,8 @@ def load(exact=False):
         "rh3t_l_vjp": (I, [V, C.c_int32, V, V, V]),
         "rh3t_adjoint_forward": (I, [V, C.c_int32, D, C.c_int32]),
         "rh3t_adjoint_backward": (I, [V, V, V, V]),
+        "rh3t_adjoint_records": (C.c_int32, [V]),
+        "rh3t_adjoint_max_records": (I, [V, C.c_int32]),
         "rh3t_snapshot": (I, [V, C.c_int32, C.c_char_p]),
         "rh3t_snapshot_wait": (I, [V]),
         "rh3t_restart": (I, [V, C.c_int32, C.c_char_p]),

@@ -677,9 +677,18 @@ class Batch(_SnapshotIO):
         self._check(self.L.rh3t_l_vjp(self.h, int(k), rb.ctypes.data, ub.ctypes.data, pb.ctypes.data))
         return ub, pb
 
-    def adjoint_forward(self, nsteps, cfl_factor=0.05, ckpt_every=20):
-        """nsteps steps of every instance with checkpoints every ckpt_every."""
+    def adjoint_forward(self, nsteps, cfl_factor=0.05, ckpt_every=20, max_records=None):
+        """nsteps steps of every instance with checkpoints every ckpt_every;
+        the last segments (as many as fit in a quarter of the free device
+        memory, at most max_records when given) are kept recorded, so the
+        reverse sweep does not recompute them."""
+        if max_records is not None:
+            self._check(self.L.rh3t_adjoint_max_records(self.h, int(max_records)))
         self._check(self.L.rh3t_adjoint_forward(self.h, int(nsteps), float(cfl_factor), int(ckpt_every)))
+
+    def adjoint_records(self):
+        """segment records the adjoint allocated"""
+        return int(self.L.rh3t_adjoint_records(self.h))
 
     def adjoint_backward(self, dJ_du, out=None):
         """dJ_du: per-instance list of (nx*ny x 6) arrays or their

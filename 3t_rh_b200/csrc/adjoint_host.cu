@@ -13,9 +13,11 @@
 //   dt = cfl dt_cfl(u0): U0 += cfl dtbar d(local dt)/du at the minimising cell,
 //   with dtbar = <r2, 2Y/3> + <r1, U2/4> + <r0, U1>;
 // and U0 is the next Y. Memory: (n_steps / ckpt_every) states plus
-// ckpt_every x (3 stage states + 3 rhs) plane sets. The forward run records
-// its last segment as it goes, so the first segment of the reverse sweep is
-// not recomputed.
+// n_rec x ckpt_every x (3 stage states + 3 rhs) plane sets. The forward run
+// records its last n_rec segments as it goes, so the reverse sweep starts
+// with n_rec segments it does not recompute: n_rec is as many records as fit
+// in a quarter of the device memory free at allocation (at least one, at most
+// the number of segments).
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -33,8 +35,10 @@ struct AdjBuffers {
     double cfl = 0.05;
     double* ckpt = nullptr;     // n_ckpt plane sets (state U at segment starts)
     DevScalars* ckpt_sc = nullptr; // n_ckpt x n_inst scalars at segment starts
-    double* seg = nullptr;      // ckpt_every x 6 plane sets: U0 U1 U2 R0 R1 R2 per step
-    DevScalars* seg_sc = nullptr; // ckpt_every x n_inst scalars (after the step's dt)
+    int n_rec = 0;              // segment records allocated
+    int max_rec = 0;            // cap on n_rec (0: the memory budget alone)
+    double* seg = nullptr;      // n_rec x ckpt_every x 6 plane sets: U0 U1 U2 R0 R1 R2 per step
+    DevScalars* seg_sc = nullptr; // n_rec x ckpt_every x n_inst scalars (after the step's dt)
     double *Y = nullptr, *U0 = nullptr, *U1 = nullptr, *U2 = nullptr, *W = nullptr, *rbar = nullptr;
     double* pbar = nullptr;     // n_inst x 8
     double* dtbar = nullptr;    // n_inst
@@ -159,6 +163,17 @@ extern "C" int rh3t_l_vjp(rh3t_ctx* c, int32_t k, const double* rbar, double* ub
     return fetch_status(c);
 }
 
+extern "C" int32_t rh3t_adjoint_records(const rh3t_ctx* c) { return c && c->adj ? c->adj->n_rec : 0; }
+
+extern "C" int rh3t_adjoint_max_records(rh3t_ctx* c, int32_t n) {
+    if (!c || n < 0) return RH3T_ERR_INVALID_ARGUMENT;
+    if (!c->adj) c->adj = new AdjBuffers();
+    c->adj->max_rec = n;
+    c->adj->n_ckpt = 0; // the next rh3t_adjoint_forward allocates again
+    c->adj->last_recorded = false;
+    return RH3T_OK;
+}
+
 extern "C" int rh3t_adjoint_forward(rh3t_ctx* c, int32_t nsteps, double cfl_factor, int32_t ckpt_every) {
     if (!c || nsteps <= 0 || ckpt_every <= 0) return RH3T_ERR_INVALID_ARGUMENT;
     CK(c, cudaSetDevice(c->device));
@@ -175,10 +190,22 @@ extern "C" int rh3t_adjoint_forward(rh3t_ctx* c, int32_t nsteps, double cfl_fact
         a->ckpt = nullptr; a->ckpt_sc = nullptr; a->seg = nullptr; a->seg_sc = nullptr;
         CK(c, cudaMalloc(&a->ckpt, (size_t)n_ckpt * np * sizeof(double)));
         CK(c, cudaMalloc(&a->ckpt_sc, (size_t)n_ckpt * ni * sizeof(DevScalars)));
-        CK(c, cudaMalloc(&a->seg, (size_t)ckpt_every * 6 * np * sizeof(double)));
-        CK(c, cudaMalloc(&a->seg_sc, (size_t)ckpt_every * ni * sizeof(DevScalars)));
+        // as many segment records as fit in a quarter of the free memory
+        const size_t rec_bytes = (size_t)ckpt_every * 6 * np * sizeof(double);
+        size_t free_b = 0, total_b = 0;
+        CK(c, cudaMemGetInfo(&free_b, &total_b));
+        int n_rec = (int)std::min<size_t>((size_t)n_ckpt, std::max<size_t>(1, free_b / 4 / rec_bytes));
+        if (a->max_rec > 0) n_rec = std::min(n_rec, a->max_rec);
+        while (n_rec > 1 && cudaMalloc(&a->seg, (size_t)n_rec * rec_bytes) != cudaSuccess) {
+            cudaGetLastError(); // an out-of-memory here only means fewer records
+            --n_rec;
+        }
+        if (n_rec == 1) CK(c, cudaMalloc(&a->seg, rec_bytes));
+        a->n_rec = n_rec;
+        CK(c, cudaMalloc(&a->seg_sc, (size_t)n_rec * ckpt_every * ni * sizeof(DevScalars)));
     }
     a->last_recorded = false;
+    const int n_rec = std::min(a->n_rec, n_ckpt);
     a->n_ckpt = n_ckpt;
     a->ckpt_every = ckpt_every;
     a->nsteps = nsteps;
@@ -194,14 +221,15 @@ extern "C" int rh3t_adjoint_forward(rh3t_ctx* c, int32_t nsteps, double cfl_fact
                               s));
         c->launches += 1;
         const int len = std::min(ckpt_every, nsteps - done);
-        if (q + 1 < n_ckpt) {
+        if (q < n_ckpt - n_rec) {
             rc = rh3t_advance(c, len, cfl_factor, INFINITY, 1);
             if (rc) return rc;
         } else {
-            // the last segment with its record (stage states, rhs, scalars)
+            // one of the last n_rec segments, with its record (stage states, rhs, scalars)
+            const size_t r = (size_t)(q - (n_ckpt - n_rec)) * ckpt_every;
             for (int j = 0; j < len; ++j) {
-                enqueue_recorded_step(c, a->seg + (size_t)j * 6 * np);
-                CK(c, cudaMemcpyAsync(a->seg_sc + (size_t)j * ni, c->d_sc, ni * sizeof(DevScalars),
+                enqueue_recorded_step(c, a->seg + (r + j) * 6 * np);
+                CK(c, cudaMemcpyAsync(a->seg_sc + (r + j) * ni, c->d_sc, ni * sizeof(DevScalars),
                                       cudaMemcpyDeviceToDevice, s));
             }
             CK(c, cudaGetLastError());
@@ -233,11 +261,15 @@ extern "C" int rh3t_adjoint_backward(rh3t_ctx* c, const double* dJ_du, double* d
     CK(c, cudaStreamSynchronize(s));
     double* final_state = a->final_state;
     launch_adj_copy(s, c->d_inst, 0, c->n_inst, mp, 0, final_state, 0);
+    const int n_rec = std::min(a->n_rec, a->n_ckpt);
+    const bool recorded = a->last_recorded;
+    a->last_recorded = false;
     for (int q = a->n_ckpt - 1; q >= 0; --q) {
         const int len = std::min(a->ckpt_every, a->nsteps - q * a->ckpt_every);
-        // recompute the segment with its record (the last one is recorded already)
-        const bool have = q == a->n_ckpt - 1 && a->last_recorded;
-        a->last_recorded = false;
+        // the last n_rec segments were recorded by the forward run; the others
+        // are recomputed into the first record
+        const bool have = recorded && q >= a->n_ckpt - n_rec;
+        const size_t r0 = have ? (size_t)(q - (a->n_ckpt - n_rec)) * a->ckpt_every : 0;
         if (!have) {
             launch_adj_copy(s, c->d_inst, 0, c->n_inst, mp, 0, a->ckpt + (size_t)q * np, 1);
             CK(c, cudaMemcpyAsync(c->d_sc, a->ckpt_sc + (size_t)q * ni, ni * sizeof(DevScalars),
@@ -252,8 +284,8 @@ extern "C" int rh3t_adjoint_backward(rh3t_ctx* c, const double* dJ_du, double* d
                                   cudaMemcpyDeviceToDevice, s));
         }
         for (int j = len - 1; j >= 0; --j) {
-            double* rec = a->seg + (size_t)j * 6 * np;
-            const DevScalars* sc = a->seg_sc + (size_t)j * ni;
+            double* rec = a->seg + (r0 + j) * 6 * np;
+            const DevScalars* sc = a->seg_sc + (r0 + j) * ni;
             CK(c, cudaMemsetAsync(a->dtbar, 0, ni * sizeof(double), s));
             launch_adj_stage(s, c->d_inst, 0, c->n_inst, c->max_cells, 2, a->Y, a->U0, a->U2, a->rbar,
                              rec + 5 * np, sc, a->dtbar);

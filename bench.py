@@ -308,6 +308,7 @@ def adjoint_bench(rh, torch, local, exact, nsteps=200, ckpt=20, n=32):
         return [(vals_h[b.offsets[k]:b.offsets[k + 1]], times_h[k]) for k in range(b.n)], out
 
     (res, (g0, gp)), a_ms, a_wall = timed(adjoint, b)
+    n_rec = b.adjoint_records()
     lib_ms = ev[0].elapsed_time(ev[1]) + ev[2].elapsed_time(ev[3])
     dmach = []
     for k, sp in enumerate(specs):
@@ -320,6 +321,10 @@ def adjoint_bench(rh, torch, local, exact, nsteps=200, ckpt=20, n=32):
                         f"omega_ei, omega_er and the initial state; checkpoints every {ckpt} steps",
             "forward_ms": f_ms, "adjoint_ms": a_ms, "adj_fwd_ratio": a_ms / f_ms,
             "adjoint_library_ms": lib_ms, "adj_fwd_ratio_library": lib_ms / f_ms,
+            "segment_records": n_rec,
+            "records_note": f"the forward run kept the records of its last {n_rec} of {-(-nsteps // ckpt)} segments "
+                            "(as many as fit in a quarter of the free device memory): the reverse sweep "
+                            "recomputes the others",
             "ratio_note": "adjoint_ms: checkpointed forward + download + host objective gradient + reverse sweep; "
                           "adjoint_library_ms: rh3t_adjoint_forward + rh3t_adjoint_backward only",
             "wall_ms": {"forward": f_wall, "adjoint": a_wall},

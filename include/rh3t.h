@@ -272,6 +272,14 @@ int rh3t_l_vjp(rh3t_ctx* ctx, int32_t k, const double* rbar, double* ubar, doubl
  * clipping) from the resident states, saving the states every ckpt_every
  * steps for rh3t_adjoint_backward. */
 int rh3t_adjoint_forward(rh3t_ctx* ctx, int32_t nsteps, double cfl_factor, int32_t ckpt_every);
+/* Segment records of the sweep (no reference counterpart): the forward run
+ * keeps the full record (stage states and rhs of every step) of its last
+ * segments, as many as fit in a quarter of the free device memory, so the
+ * reverse sweep does not recompute them. rh3t_adjoint_records: the number
+ * allocated; rh3t_adjoint_max_records: a cap (0: none) for the next
+ * rh3t_adjoint_forward, which then allocates again. */
+int32_t rh3t_adjoint_records(const rh3t_ctx* ctx);
+int rh3t_adjoint_max_records(rh3t_ctx* ctx, int32_t n);
 /* dJ_du: cotangent of the final states (all instances' value arrays
  * concatenated); dJ_du0 (out, same layout): gradient with respect to the
  * initial states; dJ_dparams (out, n x 8, may be NULL). Recomputes each

@@ -197,7 +197,8 @@ def test_gradient_vs_finite_differences(rh):
     mach, oei, oer, N = 3.0, 0.5, 2.0, 12
     J0, f, g, J = _objective(rh, mach, oei, oer, N)
     b = rh.Batch([f], [g], exact=True)
-    b.adjoint_forward(N, 0.05, ckpt_every=5)
+    b.adjoint_forward(N, 0.05, ckpt_every=5, max_records=1)  # two of the three segments recomputed
+    assert b.adjoint_records() == 1
     uN, _ = b.download(0)
     assert abs(J.value(uN) - J0) <= 1e-14 * abs(J0)
     g0, gp = b.adjoint_backward([J.grad(uN)])
@@ -273,3 +274,26 @@ def test_batch_adjoint_equals_single(rh):
         # atomic accumulation: the order of the additions differs between runs
         assert np.abs(a0[0] - g0[k]).max() <= 1e-10 * np.abs(a0[0]).max()
         assert np.abs(ap[0] - gp[k]).max() <= 1e-10 * np.abs(ap[0]).max()
+
+
+def test_segment_records_do_not_change_the_gradient(rh):
+    """The forward run keeps the records of its last segments (as many as
+    fit, or a given cap) so the reverse sweep skips their recomputation:
+    the gradients are those of the sweep that recomputes all but the last."""
+    specs = rh.cases.batch_specs(n=2, sizes=(31,))
+    fields = [rh.cases.batch_field(sp) for sp in specs]
+    grids = [rh.GhostGrid.build(f) for f in fields]
+    Js = [rh.cases.SurfacePressure(f, g) for f, g in zip(fields, grids)]
+    out = {}
+    for cap in (1, 2, 0):
+        b = rh.Batch(fields, grids, exact=True)
+        b.adjoint_forward(10, 0.05, ckpt_every=3, max_records=cap)
+        res = b.download()
+        out[cap] = (b.adjoint_records(),) + b.adjoint_backward([J.grad(u) for J, (u, _) in zip(Js, res)])
+        b.close()
+    assert out[1][0] == 1 and out[2][0] == 2 and out[0][0] == 4  # 4 segments, all fit
+    for cap in (2, 0):
+        for k in range(2):
+            a0, b0 = out[1][1][k], out[cap][1][k]
+            assert np.abs(a0 - b0).max() <= 1e-10 * np.abs(a0).max()
+        assert np.abs(out[1][2] - out[cap][2]).max() <= 1e-10 * np.abs(out[1][2]).max()
