@@ -58,3 +58,26 @@ def test_geometry_errors_reported(rh):
     f.outer_arcs[0].arc.mid = (0.0, 0.0125)  # collinear with start and end
     with pytest.raises(rh.RH3TError):
         rh.GhostGrid.build(f)
+
+
+def test_create_failure_message_without_device(rh):
+    """A failed create returns no context; its status and message are kept
+    per thread (rh3t_create_error): here, set-up on a machine without the
+    requested device, and a malformed description."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("needs a machine without a CUDA device")
+    L = rh.load()
+    f = rh.cases.init_cylinder(h=1.0 / 10.0)
+    g = rh.GhostGrid.build(f)
+    with pytest.raises(rh.RH3TError) as ei:
+        rh.Batch([f], [g])
+    assert ei.value.kind == "NO_DEVICE" and "no such CUDA device" in str(ei.value)
+    out = C.c_void_p()
+    assert L.rh3t_batch_create(1, None, 0, C.byref(out)) == 7
+    msg = C.create_string_buffer(192)
+    assert L.rh3t_create_error(msg, 192) == 0  # a null description is rejected before the record is set
+    inst = (C.c_byte * 256)()  # one instance description of null pointers
+    assert L.rh3t_batch_create(1, C.addressof(inst), 0, C.byref(out)) == 7
+    assert L.rh3t_create_error(msg, 192) == 7
+    assert msg.value.decode() == "instance 0: missing or malformed description"
