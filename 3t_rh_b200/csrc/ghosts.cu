@@ -49,7 +49,7 @@ namespace rh3t {
 constexpr int GH_WARPS = 4;
 constexpr int GH_BLOCKS_PER_SM = 3;
 constexpr int GH_PREP_THREADS = 128;
-constexpr int GH_WAIT_LIMIT = 1 << 20; // try_wait rounds before a wait counts as timed out
+constexpr int GH_WAIT_LIMIT = 1 << 18; // try_wait rounds (about a second) before a wait counts as timed out
 constexpr int GH_TIMEOUT_CODE = 11;    // RH3T_ERR_DEVICE_TIMEOUT
 __constant__ int kStOff[6] = {0, 1, 5, 14, 30, 55};
 __constant__ int kSOff[6] = {0, 1, 17, 98, 354, 979};
@@ -567,4 +567,38 @@ void launch_ghosts(cudaStream_t s, const Inst* insts, const GhostRec* heavy, int
 
 int ghost_launches(int nh, int nc) { return (nh + nc > 0 ? 1 : 0) + (nh > 0 ? 1 : 0); }
 
+// one warp: the ghost update's bounded wait on a fresh mbarrier whose phase
+// completes (arrive: one arrival, no bytes expected) or never does; out[0] =
+// 1 when the wait gave up
+__global__ void k_wait_check(int arrive, int* out) {
+    __shared__ unsigned long long bar;
+    const int lane = threadIdx.x & 31;
+    if (lane == 0) {
+        mbar_init(&bar);
+        mbar_fence_init();
+        if (arrive)
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&bar)) : "memory");
+    }
+    __syncwarp();
+    const bool ok = __all_sync(0xffffffffu, mbar_wait(&bar, 0u));
+    if (lane == 0) out[0] = ok ? 0 : 1;
+}
+
 } // namespace rh3t
+
+extern "C" int rh3t_wait_check(int32_t device, int32_t arrive, int32_t* timed_out) {
+    if (!timed_out) return 7; // RH3T_ERR_INVALID_ARGUMENT
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) return 10; // RH3T_ERR_NO_DEVICE
+    if (cudaSetDevice(device) != cudaSuccess) return 8;
+    int* d = nullptr;
+    if (cudaMalloc(&d, sizeof(int)) != cudaSuccess) return 8;
+    int h = -1;
+    rh3t::k_wait_check<<<1, 32>>>(arrive ? 1 : 0, d);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpy(&h, d, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return 8; // RH3T_ERR_CUDA
+    *timed_out = h;
+    return 0;
+}

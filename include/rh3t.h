@@ -375,6 +375,14 @@ int rh3t_fp64_peak(int32_t device, double* tflops);
  * out[3k+2] = x[k]^q. */
 int rh3t_math_check(int32_t device, const double* x, int32_t n, double q, double* out);
 
+/* Diagnostic (no reference counterpart): the bounded mbarrier wait of the
+ * ghost update (2^18 try_wait rounds, about a second on a B200, then
+ * RH3T_ERR_DEVICE_TIMEOUT) run by
+ * one warp on a barrier whose phase completes (arrive != 0) or that nothing
+ * completes (arrive == 0): *timed_out = 1 when the wait gave up, 0 when it
+ * returned with the phase complete. */
+int rh3t_wait_check(int32_t device, int32_t arrive, int32_t* timed_out);
+
 int rh3t_synchronize(rh3t_ctx* ctx);
 int rh3t_last_error(const rh3t_ctx* ctx, rh3t_error* out);
 /* status of the last rh3t_create / rh3t_batch_create on the calling thread

@@ -114,3 +114,20 @@ def test_periodic_wrap_mismatch_reported(rh):
     with pytest.raises(rh.RH3TError) as ei:
         rh.Batch([cyl, f], [rh.GhostGrid.build(cyl), g])
     assert ei.value.kind == "PERIODIC_WRAP" and "instance 1" in str(ei.value)
+
+
+@pytest.mark.gpu
+def test_bounded_wait_gives_up(rh):
+    """The ghost update's mbarrier wait is bounded (RH3T_ERR_DEVICE_TIMEOUT
+    instead of a hang): on a barrier that nothing completes it gives up, on
+    one whose phase completes it returns, and the device stays usable."""
+    import ctypes as C
+    import time
+    L = rh.load()
+    t = C.c_int32(-1)
+    assert L.rh3t_wait_check(0, 1, C.byref(t)) == 0 and t.value == 0
+    t0 = time.perf_counter()
+    assert L.rh3t_wait_check(0, 0, C.byref(t)) == 0 and t.value == 1
+    print(f"wait gave up after {time.perf_counter() - t0:.3f} s")
+    assert time.perf_counter() - t0 < 30.0
+    assert L.rh3t_wait_check(0, 1, C.byref(t)) == 0 and t.value == 0
