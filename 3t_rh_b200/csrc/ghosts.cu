@@ -48,7 +48,7 @@ namespace rh3t {
 
 constexpr int GH_WARPS = 4;
 constexpr int GH_BLOCKS_PER_SM = 3;
-constexpr int GH_PREP_THREADS = 128;
+constexpr int GH_PREP_THREADS = 64; // 41.6 KB of staging per block: 5 blocks per SM
 constexpr int GH_WAIT_LIMIT = 1 << 18; // try_wait rounds (about a second) before a wait counts as timed out
 constexpr int GH_TIMEOUT_CODE = 11;    // RH3T_ERR_DEVICE_TIMEOUT
 __constant__ int kStOff[6] = {0, 1, 5, 14, 30, 55};
