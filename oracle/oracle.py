@@ -3,7 +3,8 @@
 ctypes front end of the CPU restatement of colinhu123/3T_RH's hot path
 (``oracle/src``). Only ``tests/``, ``__graft_entry__.smoke()`` and the
 ``cpu_baseline`` / ``--impl reference`` legs of ``bench.py`` may use it, and
-only as the checker or the timed CPU baseline; the product never imports it.
+only as the reference values of parity tests or the timed CPU baseline; the
+product never imports it.
 """
 import ctypes as C
 import os

@@ -1,4 +1,4 @@
-"""Test infrastructure (the checker, not the product): a numpy restatement of
+"""Test infrastructure (reference values for tests, not the product): a numpy restatement of
 the reference's RH3TBIN1 snapshot writer and reader (src/io.rs:1-123) and of
 its energy-split tool (py_utils/energy_split.py:12-31), used to check the
 library's device-packed snapshots, its restart path and its device

@@ -32,7 +32,7 @@ def test_cylinder_reference_grid(rh, O):
     oc = O.Case.cylinder()
     assert np.array_equal(f.value, oc.state())
     g = _compare(rh, O, f, oc)
-    # SURVEY-independent counts of the reference case (121 x 481)
+    # counts of the reference case (121 x 481): fluid nodes, ghosts, heavy ghosts
     assert f.fluid.sum() == 55132 and g.len() == 4914 and g.n_heavy() == 4480
 
 

@@ -1,4 +1,4 @@
-"""The oracle's dual-number l() (oracle/src/jvp.hpp), the checker of the
+"""The oracle's dual-number l() (oracle/src/jvp.hpp), the reference values of the
 CUDA adjoint: its double instantiation reproduces the oracle's l() bit for
 bit, its value parts do too, its tangent is linear in the direction, and it
 matches central differences in the exchange coefficients (a direction that
