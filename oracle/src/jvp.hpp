@@ -6,7 +6,7 @@
 // (same operations in the same order) and the tangent parts give the
 // directional derivative J_l(u) du of l() for a state direction du, a
 // FarField state direction and exchange-coefficient directions. It is the
-// checker of the CUDA adjoint (vector-Jacobian products).
+// reference of the CUDA adjoint (vector-Jacobian products) in the tests.
 #pragma once
 #include "model.hpp"
 #include <cmath>

@@ -1,5 +1,5 @@
 // ORACLE — test infrastructure only. CPU restatement of the 3T_RH pointwise
-// physics and interface operators, used as the parity checker for the CUDA
+// physics and interface operators, used as the parity reference for the CUDA
 // path and as the timed CPU baseline. Product code never links this.
 //
 // Every function follows the reference Rust source operation for operation
