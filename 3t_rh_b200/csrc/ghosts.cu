@@ -345,7 +345,7 @@ __device__ __forceinline__ void dot_pair(GhostWarp& G, const double* __restrict_
     const double* __restrict__ p1 = row_src(rec, c1, m, st1);
     const double* __restrict__ p2 = row_src(rec, c2, m, st2);
     double a1[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, a2[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-#pragma unroll 2
+#pragma unroll 4
     for (int b = 0; b < m; ++b) {
         const double x1 = p1[b * st1], x2 = p2[b * st2];
         double d[6];
