@@ -17,16 +17,35 @@ _LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
 _lib = None
 
 
+_VARIANTS = {}
+
+
+def _variant(libname):
+    if libname not in _VARIANTS:
+        import importlib.util
+        spec = importlib.util.spec_from_file_location(f"oracle_variant_{libname}", os.path.abspath(__file__))
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        mod._LIB_PATH = os.path.join(_HERE, "_build", libname)
+        _VARIANTS[libname] = mod
+    return _VARIANTS[libname]
+
+
 def fma_variant():
     """A second instance of this module bound to liboracle_fma.so (the
     restatement compiled with FMA contraction): the rounding envelope of the
     reference algorithm."""
-    import importlib.util
-    spec = importlib.util.spec_from_file_location("oracle_fma_variant", os.path.abspath(__file__))
-    mod = importlib.util.module_from_spec(spec)
-    spec.loader.exec_module(mod)
-    mod._LIB_PATH = os.path.join(_HERE, "_build", "liboracle_fma.so")
-    return mod
+    return _variant("liboracle_fma.so")
+
+
+def crpow_variant():
+    """This module bound to liboracle_crpow.so: the restatement (no
+    contraction) with the correctly rounded power in place of libm pow for
+    the reference's two powf calls (state.rs:261, bc1.rs:241). Its distance
+    from the plain oracle is how far a last-bit change of libm moves a run;
+    on runs it moves, it is the parity reference of the no-contraction CUDA
+    build, which computes the same correctly rounded power."""
+    return _variant("liboracle_crpow.so")
 
 # Order of the 15 runtime parameters (oracle/src/physics.hpp Params)
 PARAM_NAMES = ("gamma_e", "gamma_i", "gamma_r", "cve", "cvi", "a_rad", "kappa_e", "kappa_i", "kappa_r",

@@ -41,6 +41,72 @@ template <class T> inline T powi(T a, int b) {
     return recip ? T(1.0) / r : r;
 }
 template <class T> inline T sq(T x) { return x * x; }            // powi(x, 2)
+
+// Rust `powf` (state.rs:261 x^0.25, bc1.rs:241 x^WENO_Q) is libm pow: glibc's
+// is within 0.52 ulp and not always correctly rounded. Built with
+// -DORACLE_CRPOW the restatement takes the correctly rounded power instead
+// (double-double products, Dekker 1971), the power the CUDA path computes:
+// that build separates what a last-bit change of libm does to a run from
+// every other difference.
+#ifdef ORACLE_CRPOW
+struct DDPair {
+    double hi, lo;
+};
+inline DDPair dd_product(DDPair a, DDPair b) {
+    double p = a.hi * b.hi;
+    double e = std::fma(a.hi, b.hi, -p);
+    e = std::fma(a.hi, b.lo, e);
+    e = std::fma(a.lo, b.hi, e);
+    double s = p + e;
+    return {s, e - (s - p)};
+}
+inline DDPair dd_square(double a) { // exact: a*a = hi + lo
+    double p = a * a;
+    return {p, std::fma(a, a, -p)};
+}
+inline double cr_int_power(double x, int n) { // n >= 1, binary powering in double-double
+    if (!std::isfinite(x) || x == 0.0) return std::pow(x, (double)n);
+    DDPair r = {1.0, 0.0}, a = {x, 0.0};
+    bool first = true;
+    while (n > 0) {
+        if (n & 1) {
+            r = first ? a : dd_product(r, a);
+            first = false;
+        }
+        n >>= 1;
+        if (n) a = (a.lo == 0.0) ? dd_square(a.hi) : dd_product(a, a);
+    }
+    if (!std::isfinite(r.hi)) return r.hi;
+    return r.hi + r.lo;
+}
+inline double cr_quarter_power(double x) { // of sqrt(sqrt(x)) and its neighbours, the one whose 4th power is nearest x
+    double y = std::sqrt(std::sqrt(x));
+    if (!(x > 0.0) || !std::isfinite(x) || !std::isfinite(y)) return y;
+    double cand[3] = {std::nextafter(y, 0.0), y, std::nextafter(y, INFINITY)};
+    double best = y, bd = INFINITY;
+    for (int k = 0; k < 3; ++k) {
+        DDPair c2 = dd_square(cand[k]);
+        DDPair c4 = dd_product(c2, c2);
+        double d = std::fabs((c4.hi - x) + c4.lo);
+        if (d < bd || (d == bd && k == 1)) {
+            bd = d;
+            best = cand[k];
+        }
+    }
+    return best;
+}
+#endif
+template <class T> inline T powf_ref(T x, double p) {
+    using std::pow;
+    return pow(x, p);
+}
+#ifdef ORACLE_CRPOW
+template <> inline double powf_ref<double>(double x, double p) {
+    if (p == 0.25) return cr_quarter_power(x);
+    if (p >= 1.0 && p <= 64.0 && p == std::floor(p)) return cr_int_power(x, (int)p);
+    return std::pow(x, p);
+}
+#endif
 template <class T> inline T pow4(T x) { return (x * x) * (x * x); } // powi(x, 4)
 
 enum Dir { DIR_X = 0, DIR_Y = 1 };
@@ -73,7 +139,7 @@ template <class T> inline DerivedT<T> derived_from_state(const StateT<T>& s, con
     d.te = s.ee / (s.rho * P.cve) - w2 / (6.0 * P.cve);
     d.ti = s.ei / (s.rho * P.cvi) - w2 / (6.0 * P.cvi);
     T er_term = s.er / s.rho - w2 / 6.0;
-    d.tr = pow(er_term * s.rho / P.a_rad, 0.25);
+    d.tr = powf_ref(er_term * s.rho / P.a_rad, 0.25);
     return d;
 }
 
@@ -335,7 +401,7 @@ template <class T> inline T state_tr(const StateT<T>& s, const Params& P) {
     using std::pow;
     T u = s.mx / s.rho, v = s.my / s.rho;
     T er = s.er / s.rho - (sq(u) + sq(v)) / 6.0;
-    return pow(er * s.rho / P.a_rad, 0.25);
+    return powf_ref(er * s.rho / P.a_rad, 0.25);
 }
 
 // source.rs:7-21

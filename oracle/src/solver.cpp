@@ -117,7 +117,7 @@ static void weno_extrapolation_all(const double L[6][6], const GhostBC& bc, cons
                 }
                 vks[k][c][r] = vk;
             }
-            alpha[c][r] = bc.d[r] / std::pow(P.eps + beta, P.weno_q);
+            alpha[c][r] = bc.d[r] / powf_ref(P.eps + beta, P.weno_q);
             asum[c] += alpha[c][r];
         }
     }
@@ -738,7 +738,7 @@ static void weno_extrapolation_all_t(const T L[6][6], const GhostBC& bc, const S
                 }
                 vks[k][c][r] = vk;
             }
-            alpha[c][r] = bc.d[r] / pow(P.eps + beta, P.weno_q);
+            alpha[c][r] = bc.d[r] / powf_ref(P.eps + beta, P.weno_q);
             asum[c] += alpha[c][r];
         }
     }
