@@ -121,6 +121,9 @@ def lib():
             ("oracle_ghost_extrapolation", I, [P, LG, dp]),
             ("oracle_ghost_id", LG, [P, LG, LG]),
             ("oracle_flop_counts", None, [C.c_void_p]),
+            ("oracle_reconstruction_slow", None, [dp, I, I, dp, dp]),
+            ("oracle_ghost_probe", I, [P, LG, LG, dp]),
+            ("oracle_ghost_value_at", I, [P, LG, LG, dp, I, I, I, dp]),
         ]:
             f = getattr(L, name)
             f.restype = res
@@ -342,6 +345,26 @@ class Case:
             raise OracleError(-n, "cannot fit paper substencil", (0, 0))
         return out
 
+    def ghost_probe(self, i, j):
+        """(projection[5], side) of grid point (i, j) on the outer polygon, as
+        the reference's ghost_bc_fast_matches_slow forms them (main.rs:567-596)."""
+        proj = np.zeros(5)
+        side = lib().oracle_ghost_probe(self.h, i, j, _dp(proj))
+        return proj, side
+
+    def ghost_value_at(self, i, j, proj5, side, boundary=0, mode="fast"):
+        """set_ghost_point_value at (i, j) for the given projection and side on
+        the current state: mode "fast" (precomputed GhostBC, bc1.rs:108-255),
+        "slow" (per-call least squares, bc1.rs:345-421) or "slow_beta0" (the
+        per-call path with the precomputed path's r = 0 indicator)."""
+        out = np.zeros(6)
+        p = np.asarray(proj5, dtype=np.float64)
+        rc = lib().oracle_ghost_value_at(self.h, i, j, _dp(p), boundary, side,
+                                         {"fast": 0, "slow": 1, "slow_beta0": 2}[mode], _dp(out))
+        if rc:
+            raise OracleError(rc, "ghost value", (i, j))
+        return out
+
     def project_outer(self, x, y):
         out = np.zeros(5)
         lib().oracle_project_outer(self.h, x, y, _dp(out))
@@ -400,6 +423,15 @@ def reconstruction(pts, direction, recon=True, params=None):
     p = params if params is not None else params_array()
     out = np.zeros(6)
     lib().oracle_reconstruction(_dp(a), direction, int(recon), _dp(p), _dp(out))
+    return out
+
+
+def reconstruction_slow(pts, direction, recon=True, params=None):
+    """weno.rs:599-679 Stencil6::reconstruction (ndarray L/R, State::flux)"""
+    a = np.ascontiguousarray(pts, dtype=np.float64).reshape(36)
+    p = params if params is not None else params_array()
+    out = np.zeros(6)
+    lib().oracle_reconstruction_slow(_dp(a), direction, int(recon), _dp(p), _dp(out))
     return out
 
 

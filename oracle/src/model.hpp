@@ -176,6 +176,17 @@ void precompute_ghost_bc(const Projection& p, const Field& f, const Matrix forms
 std::vector<double> fit_polynomial_surface(const std::vector<std::array<double, 3>>& data, int degree);
 double x_derivative_at_origin(const std::vector<double>& c, int degree, int k);
 
+// bc1.rs:294-312 build_local_plain (solver.cpp)
+void build_local_plain(Vec2 n, const State& val, const Params& P, double L[6][6], double R[6][6], double lam[6]);
+// bc1.rs:676-928 Wall / Outflow / FarField rows + Taylor sum (solver.cpp)
+State ghost_from_extrapolation(const BC& bc, const Projection& pr, const double L[6][6], const double R[6][6],
+                               const double lam[6], const double v[5][6], const Params& P, long gi, long gj);
+
+// slowpath.cpp: weno.rs:599-679 reconstruction; bc1.rs:345-421 weno_extrapolation
+State reconstruction_slow(const State pts[6], Dir dir, bool recon_type, const Params& P);
+void weno_extrapolation_slow(const Projection& pr, const Field& f, const State* val, const Params& P, int k,
+                             bool beta0_as_fast, double out[6]);
+
 struct OracleError : std::runtime_error {
     int code;
     long i, j;

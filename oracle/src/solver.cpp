@@ -70,7 +70,7 @@ static void build_ilw_row1(const double u0[6], const Params& P, double row[6]) {
 
 // bc1.rs:294-312 build_local_plain: L, R, lambda at the nearest fluid node,
 // state rotated to the (normal, tangential) frame, X-direction matrices.
-static void build_local_plain(Vec2 n, const State& val, const Params& P, double L[6][6], double R[6][6], double lam[6]) {
+void build_local_plain(Vec2 n, const State& val, const Params& P, double L[6][6], double R[6][6], double lam[6]) {
     double mom_n = val.mx * n.x + val.my * n.y;
     double mom_t = -val.mx * n.y + val.my * n.x;
     State s1{val.rho, mom_n, mom_t, val.ee, val.ei, val.er};
@@ -208,6 +208,15 @@ static State set_ghost_point_value(const GhostInfo& g, const Field& f, const Sta
     build_local_plain(pr.normal, val[f.linear_index(pre.nearest_i, pre.nearest_j)], P, L, R, lam);
     double v[5][6];
     weno_extrapolation_all(L, pre, val, P, v);
+    return ghost_from_extrapolation(bc, pr, L, R, lam, v, P, g.i, g.j);
+}
+
+// bc1.rs:676-928: the Wall / Outflow / FarField rows from the extrapolated
+// characteristic derivatives v[k] (k = 0..4) and L, R, lambda at the nearest
+// node, then the Taylor sum to the ghost point (shared by the precomputed
+// path above and the per-call path of slowpath.cpp, as in the reference).
+State ghost_from_extrapolation(const BC& bc, const Projection& pr, const double L[6][6], const double R[6][6],
+                               const double lam[6], const double v[5][6], const Params& P, long gi, long gj) {
     double u[5][6];
     if (bc.kind == BC_WALL) {
         // bc1.rs:691-756
@@ -216,7 +225,7 @@ static State set_ghost_point_value(const GhostInfo& g, const Field& f, const Sta
         for (int c = 0; c < 6; ++c) A0[0][c] = c == 1 ? 1.0 : 0.0;
         for (int c = 0; c < 6; ++c) rhs0[c] = v[0][c];
         rhs0[0] = 0.0;
-        if (!solve6(A0, rhs0)) throw OracleError(ERR_SINGULAR, "singular ILW/extrapolation system at boundary", g.i, g.j);
+        if (!solve6(A0, rhs0)) throw OracleError(ERR_SINGULAR, "singular ILW/extrapolation system at boundary", gi, gj);
         for (int c = 0; c < 6; ++c) u[0][c] = rhs0[c];
         double A1[6][6], rhs1[6], row1[6];
         std::memcpy(A1, L, sizeof(A1));
@@ -224,7 +233,7 @@ static State set_ghost_point_value(const GhostInfo& g, const Field& f, const Sta
         for (int c = 0; c < 6; ++c) A1[0][c] = row1[c];
         for (int c = 0; c < 6; ++c) rhs1[c] = v[1][c];
         rhs1[0] = 0.0;
-        if (!solve6(A1, rhs1)) throw OracleError(ERR_SINGULAR, "singular ILW/extrapolation system at boundary", g.i, g.j);
+        if (!solve6(A1, rhs1)) throw OracleError(ERR_SINGULAR, "singular ILW/extrapolation system at boundary", gi, gj);
         for (int c = 0; c < 6; ++c) u[1][c] = rhs1[c];
         for (int k = 2; k <= 4; ++k) mat_vec(R, v[k], u[k]);
     } else if (bc.kind == BC_OUTFLOW) {
@@ -1332,6 +1341,79 @@ int oracle_ghost_extrapolation(void* h, long id, double* v30) {
     weno_extrapolation_all(L, pre, s.f.value.data(), s.P, v);
     std::memcpy(v30, v, sizeof(v));
     return 0;
+}
+// weno.rs:599-679 Stencil6::reconstruction (the ndarray variant)
+void oracle_reconstruction_slow(const double* pts36, int dir, int recon, const double* params, double* out6) {
+    Params P;
+    params_from(params, P);
+    State pts[6];
+    for (int i = 0; i < 6; ++i)
+        for (int k = 0; k < 6; ++k) pts[i][k] = pts36[6 * i + k];
+    State r = reconstruction_slow(pts, (Dir)dir, recon != 0, P);
+    for (int k = 0; k < 6; ++k) out6[k] = r[k];
+}
+// The projection and side main.rs:567-596 give grid point (i, j) on the outer
+// polygon: raw projection, BC-priority side, arc override or side geometry.
+int oracle_ghost_probe(void* h, long i, long j, double* proj5) {
+    const Field& f = ((Handle*)h)->s.f;
+    Point p{f.grid.x(i), f.grid.y(j)};
+    Projection raw = project_polygon(f.outer, p);
+    size_t side = select_boundary_side(raw.point, f.outer, f.bc_outer);
+    Projection pr;
+    if (const CircularArc* arc = f.arc_for_side(OUTER, side)) {
+        pr = arc->project(p);
+    } else {
+        Vec2 n = f.outer.outward_normal_of_side(side);
+        double dx = p.x - raw.point.x, dy = p.y - raw.point.y;
+        pr = {raw.point, n, dx * n.x + dy * n.y};
+    }
+    proj5[0] = pr.point.x; proj5[1] = pr.point.y; proj5[2] = pr.normal.x; proj5[3] = pr.normal.y;
+    proj5[4] = pr.distance;
+    return (int)side;
+}
+// set_ghost_point_value (bc1.rs:609-928) at grid point (i, j) with a given
+// projection, boundary and side, on the handle's current state and time.
+// mode 0: the precomputed path (precompute_ghost_bc for this projection,
+// bc1.rs:108-188, then weno_extrapolation_pre); mode 1: the per-call path
+// (bc1.rs:345-421); mode 2: the per-call path with the precomputed path's
+// r = 0 smoothness indicator (2 h^2 v^2).
+int oracle_ghost_value_at(void* h, long i, long j, const double* proj5, int boundary, int side, int mode,
+                          double* out6) {
+    Solver& s = ((Handle*)h)->s;
+    const Field& f = s.f;
+    GhostInfo g;
+    g.i = i; g.j = j;
+    g.project = {{proj5[0], proj5[1]}, {proj5[2], proj5[3]}, proj5[4]};
+    g.boundary = (BoundaryKind)boundary;
+    g.side_id = (size_t)side;
+    find_nearest_grid_point(g.project, f, g.nearest_i, g.nearest_j);
+    const BC& bc = (g.boundary == OUTER ? f.bc_outer : f.bc_inner)[g.side_id];
+    try {
+        State r;
+        if (bc.kind != BC_WALL && bc.kind != BC_OUTFLOW && bc.kind != BC_FAR_FIELD) {
+            r = set_ghost_point_value(g, f, f.value.data(), f.time, s.gg, s.P);
+        } else {
+            double L[6][6], R[6][6], lam[6], v[5][6];
+            if (mode == 0) {
+                double hh = std::sqrt(f.grid.dx * f.grid.dy);
+                Matrix forms[5];
+                for (int q = 0; q < 5; ++q) forms[q] = beta_quadratic_form(q, hh);
+                GhostBC pre;
+                precompute_ghost_bc(g.project, f, forms, pre);
+                build_local_plain(g.project.normal, f.value[f.linear_index(pre.nearest_i, pre.nearest_j)], s.P, L, R,
+                                  lam);
+                weno_extrapolation_all(L, pre, f.value.data(), s.P, v);
+            } else {
+                build_local_plain(g.project.normal, f.value[f.linear_index(g.nearest_i, g.nearest_j)], s.P, L, R,
+                                  lam);
+                for (int k = 0; k < 5; ++k)
+                    weno_extrapolation_slow(g.project, f, f.value.data(), s.P, k, mode == 2, v[k]);
+            }
+            r = ghost_from_extrapolation(bc, g.project, L, R, lam, v, s.P, i, j);
+        }
+        for (int k = 0; k < 6; ++k) out6[k] = r[k];
+        return 0;
+    } catch (OracleError& e) { return e.code; }
 }
 long oracle_ghost_id(void* h, long i, long j) {
     GhostGrid& gg = ((Handle*)h)->s.gg;

@@ -83,23 +83,29 @@ def test_x_and_y_flux_are_direction_sensitive(O):  # weno.rs:1287-1317
     assert abs(fx[0] - s[1]) < TOL and abs(fy[0] - s[2]) < TOL
 
 
-def test_reconstruction_lcg_stencils_finite(O):
-    """main.rs:493-545 draws 100 stencils from its LCG (seed 12345) to compare
-    the fast and the ndarray reconstruction; there is one reconstruction in the
-    restatement, so the same stencils check finiteness and the recon-type
-    switch instead."""
+def test_reconstruction_fast_matches_reconstruction(O):
+    """main.rs:514-545: 100 stencils from the test's LCG (main.rs:493-498, seed
+    12345; rho in [0.5, 1.5], momenta in [-0.5, 0.5], energies in [1, 2]),
+    reconstruction_fast (weno.rs:685-802) against the ndarray reconstruction
+    (weno.rs:599-679) for both recon types and directions, max abs difference
+    < 1e-12."""
     seed = [12345]
 
     def rng():
         seed[0] = (seed[0] * 6364136223846793005 + 1442695040888963407) & 0xFFFFFFFFFFFFFFFF
         return float(seed[0] >> 11) / float(1 << 53)
 
+    worst = 0.0
     for _ in range(100):
         pts = np.array([[0.5 + rng(), rng() - 0.5, rng() - 0.5, 1.0 + rng(), 1.0 + rng(), 1.0 + rng()]
                         for _ in range(6)])
-        for d in (X, Y):
-            for recon in (True, False):
-                assert np.isfinite(O.reconstruction(pts, d, recon)).all()
+        for recon in (True, False):
+            for d in (X, Y):
+                a = O.reconstruction_slow(pts, d, recon)
+                b = O.reconstruction(pts, d, recon)
+                assert np.isfinite(b).all()
+                worst = max(worst, np.abs(a - b).max())
+    assert worst < 1e-12
 
 
 # ------------------------------------------------------------------ noncon.rs tests
