@@ -19,7 +19,7 @@ EXPORTS = (
     "rh3t_geom_ghost_table",
     "rh3t_geom_access_table", "rh3t_geom_last_error", "rh3t_geom_destroy", "rh3t_default_params", "rh3t_create",
     "rh3t_upload_state", "rh3t_download_state", "rh3t_l", "rh3t_calc_global_dt", "rh3t_rk3_ssp", "rh3t_advance",
-    "rh3t_step_host", "rh3t_last_dt", "rh3t_profile_steps", "rh3t_fp64_peak", "rh3t_math_check",
+    "rh3t_step_host", "rh3t_last_dt", "rh3t_profile_steps", "rh3t_fp64_peak", "rh3t_math_check", "rh3t_div_check",
     "rh3t_calc_global_dt_noalloc", "rh3t_synchronize", "rh3t_last_error", "rh3t_create_error", "rh3t_wait_check", "rh3t_step_host_batch", "rh3t_kernel_launches", "rh3t_stream",
     "rh3t_destroy", "rh3t_batch_create", "rh3t_instance_count", "rh3t_upload_batch", "rh3t_download_batch",
     "rh3t_upload_instance", "rh3t_download_instance", "rh3t_l_instance", "rh3t_calc_global_dt_batch",
@@ -118,6 +118,7 @@ def load(exact=False):
         "rh3t_profile_steps": (I, [V, C.c_int32, D, V, V]),
         "rh3t_fp64_peak": (I, [C.c_int32, P(D)]),
         "rh3t_math_check": (I, [C.c_int32, V, C.c_int32, D, V]),
+        "rh3t_div_check": (I, [C.c_int32, C.c_int64, C.c_uint64, V, V]),
         "rh3t_calc_global_dt_noalloc": (I, [P(Grid), P(Params), V, V, V, V]),
         "rh3t_synchronize": (I, [V]),
         "rh3t_last_error": (I, [V, P(Error)]),

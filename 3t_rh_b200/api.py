@@ -421,9 +421,14 @@ class _SnapshotIO:
 
 class Solver(_SnapshotIO):
     """Device copy of a Field + GhostGrid + the l() scratch (main.rs:45-67):
-    one rh3t_ctx on one CUDA stream."""
+    one rh3t_ctx on one CUDA stream.
 
-    def __init__(self, field, ghosts, device=0, exact=False):
+    exact=True (default): librh3t_exact, the reference's expressions and
+    roundings (no FMA contraction, IEEE quotients, correctly rounded pow);
+    exact=False: librh3t, FMA contraction and shared reciprocals (faster; its
+    roundings differ from the reference's by a few ulps per operation)."""
+
+    def __init__(self, field, ghosts, device=0, exact=True):
         self.L = _lib.load(exact)
         self.exact = exact
         self.grid = field.grid
@@ -524,7 +529,7 @@ class Batch(_SnapshotIO):
     whole batch. No reference counterpart: the reference runs one Field per
     process."""
 
-    def __init__(self, fields, ghostgrids, device=0, exact=False):
+    def __init__(self, fields, ghostgrids, device=0, exact=True):
         if len(fields) != len(ghostgrids) or not fields:
             raise ValueError("one GhostGrid per Field, at least one")
         self.L = _lib.load(exact)

@@ -36,7 +36,10 @@ __device__ __forceinline__ double weno5_any(double a, double b, double c, double
     return fastm::weno5(a, b, c, d, e, eps);
 }
 
-constexpr int NQ = 15; // Roe state: u v w2 ee ei er cs2 cs he hi hr b den, 1/cs2, 1/b
+// Roe state: u v w2 ee ei er cs2 cs he hi hr b den, then the reciprocals
+// the L rows divide by: FMA build 1/cs2, 1/b; no-contraction build RN(1/d)
+// of d = den, b, 6 cs2, 3 cs2, gt cs2 (their quotients stay the IEEE ones)
+constexpr int NQ = 18;
 
 struct FluxShared {
     double2 U[3][FLUX_NPT]; // (rho, mx), (my, ee), (ei, er)
@@ -65,13 +68,25 @@ __device__ __forceinline__ void load_q(const FluxShared& S, int f, Roe& q, doubl
 }
 
 template <int DIR>
-__device__ __forceinline__ double char_flux(const FluxShared& S, const DevParams& P, int c, int f, int p0, int ps) {
+__device__ __forceinline__ double char_flux(const FluxShared& S, const DevParams& P, const Recip& rgt, int c, int f,
+                                            int p0, int ps) {
     Roe q;
     double ics2, ib;
     load_q(S, f, q, ics2, ib);
     double Lc[6];
-    if (kExact) l_row<DIR>(c, q, P, Lc);
-    else fastm::l_row<DIR>(c, q, ics2, ib, P, Lc);
+    if (kExact) {
+        RoeDiv rd;
+        const double gt = (P.gamma_i - 1.0) + (P.gamma_e - 1.0) + (P.gamma_r - 1.0);
+        rd.den = recip_of(q.den, S.Q[13][f]);
+        rd.b = recip_of(q.b, S.Q[14][f]);
+        rd.c6 = recip_of(6.0 * q.cs2, S.Q[15][f]);
+        rd.c3 = recip_of(3.0 * q.cs2, S.Q[16][f]);
+        rd.cg = recip_of(gt * q.cs2, S.Q[17][f]);
+        rd.gt = rgt;
+        l_row<DIR>(c, q, rd, P, Lc);
+    } else {
+        fastm::l_row<DIR>(c, q, ics2, ib, P, Lc);
+    }
     const double vel = DIR == 0 ? q.u : q.v;
     const double lam = c == 0 ? vel - q.cs : (c == 5 ? vel + q.cs : vel);
     const double a = fabs(lam);
@@ -181,14 +196,23 @@ __device__ __forceinline__ void flux_tile(const Inst& I, const Tile& t, int stag
                 const double b6[6] = {sqrt(s2[0]), d2.u, d2.v, d2.e_e, d2.e_i, d2.e_r};
                 q = fastm::roe(a6, b6, P);
             }
-            const double qv[NQ] = {q.u, q.v, q.w2, q.ee, q.ei, q.er, q.cs2, q.cs, q.he, q.hi, q.hr, q.b, q.den,
-                                   kExact ? 0.0 : 1.0 / q.cs2, kExact ? 0.0 : 1.0 / q.b};
+            double qv[NQ] = {q.u, q.v, q.w2, q.ee, q.ei, q.er, q.cs2, q.cs, q.he, q.hi, q.hr, q.b, q.den,
+                             0.0, 0.0, 0.0, 0.0, 0.0};
+            if (kExact) {
+                const RoeDiv rd = roe_div(q, P);
+                qv[13] = rd.den.y; qv[14] = rd.b.y; qv[15] = rd.c6.y; qv[16] = rd.c3.y; qv[17] = rd.cg.y;
+            } else {
+                qv[13] = 1.0 / q.cs2;
+                qv[14] = 1.0 / q.b;
+            }
 #pragma unroll
             for (int k = 0; k < NQ; ++k) S.Q[k][f] = qv[k];
         }
     }
     __syncthreads();
     const int c = threadIdx.x >> 5, lane = threadIdx.x & 31; // warp-uniform characteristic field
+    Recip rgt = {1.0, 1.0, false};
+    if (kExact) rgt = recip((P.gamma_i - 1.0) + (P.gamma_e - 1.0) + (P.gamma_r - 1.0));
     // ---- 2. characteristic pass: field c of faces lane and lane + 32
 #pragma unroll
     for (int h = 0; h < FLUX_FACES / 32; ++h) {
@@ -196,7 +220,7 @@ __device__ __forceinline__ void flux_tile(const Inst& I, const Tile& t, int stag
         if (S.act[f]) {
             int i, j, p0, ps;
             face_index<DIR>(t, f, i, j, p0, ps);
-            S.G[c][f] = char_flux<DIR>(S, P, c, f, p0, ps);
+            S.G[c][f] = char_flux<DIR>(S, P, rgt, c, f, p0, ps);
         }
     }
     __syncthreads();
@@ -208,8 +232,14 @@ __device__ __forceinline__ void flux_tile(const Inst& I, const Tile& t, int stag
     }
 }
 
-// 64 registers: 5 blocks (30 warps) per SM instead of 4 at the uncapped 76
-__global__ void __launch_bounds__(FLUX_THREADS, 5) k_flux(const Inst* __restrict__ insts, const Tile* __restrict__ tx,
+// FMA build: 64 registers, 5 blocks (30 warps) per SM instead of 4 at the
+// uncapped 76. No-contraction build: 80 registers, 4 blocks (its divisions
+// by shared reciprocals keep more values live; at 64 it spills).
+#ifndef FLUX_MIN_BLOCKS_EXACT
+#define FLUX_MIN_BLOCKS_EXACT 4
+#endif
+constexpr int FLUX_MIN_BLOCKS = kExact ? FLUX_MIN_BLOCKS_EXACT : 5;
+__global__ void __launch_bounds__(FLUX_THREADS, FLUX_MIN_BLOCKS) k_flux(const Inst* __restrict__ insts, const Tile* __restrict__ tx,
                                                        int ntx, const Tile* __restrict__ ty, int nty, int stage) {
     __shared__ FluxShared S;
     const int b = blockIdx.x;

@@ -432,9 +432,10 @@ __device__ __forceinline__ void heavy_ghost(const Inst* __restrict__ insts, cons
         const int k = lane / 6, c = lane - 6 * (lane / 6);
         double asum = 0.0;
         for (int r = 0; r < 5; ++r) asum += G.alpha[c][r];
+        const Recip ra = recip(asum); // five quotients by one divisor (IEEE results, divrn.cuh)
         double res = 0.0;
         for (int r = 0; r < 5; ++r)
-            res += (G.alpha[c][r] / asum) * (k <= r ? G.V[c][r * (r + 1) / 2 + k] : 0.0);
+            res += div_rn(G.alpha[c][r], ra) * (k <= r ? G.V[c][r * (r + 1) / 2 + k] : 0.0);
         G.v[k][c] = res;
     }
     __syncwarp();

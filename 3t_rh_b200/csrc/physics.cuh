@@ -6,6 +6,7 @@
 // mul+add -> FMA contraction (disabled in the RH3T_EXACT build).
 #pragma once
 #include "rh3t_dev.h"
+#include "divrn.cuh"
 
 namespace rh3t {
 
@@ -71,33 +72,45 @@ __device__ __forceinline__ double pow_q(double x, double q) {
     return pow(x, q);
 }
 
+// x / 3 and x / 6 written once for every scalar type: the IEEE quotient by
+// divrn.cuh for double, the type's own division otherwise (dual numbers)
+__device__ __forceinline__ double quot3(double x) { return div3_rn(x); }
+__device__ __forceinline__ double quot6(double x) { return div6_rn(x); }
+template <class T> __device__ __forceinline__ T quot3(const T& x) { return x / 3.0; }
+template <class T> __device__ __forceinline__ T quot6(const T& x) { return x / 6.0; }
+
 // Subset of state.rs:245-276 Derived::from_state needed by fluxes, L/R and noncon.
 struct Prim {
     double u, v, e_e, e_i, e_r, pe, pi, pr;
 };
 
+// Every quotient is the IEEE one (divrn.cuh): the five by rho share one
+// reciprocal, w2 / 6 and rho w2 / 6 are each formed once.
 __device__ __forceinline__ Prim prim_from_state(const double s[6], const DevParams& P) {
     Prim d;
-    d.u = s[1] / s[0];
-    d.v = s[2] / s[0];
+    const Recip r0 = recip(s[0]);
+    d.u = div_rn(s[1], r0);
+    d.v = div_rn(s[2], r0);
     double w2 = sqd(d.u) + sqd(d.v);
-    d.e_e = s[3] / s[0] - w2 / 6.0;
-    d.e_i = s[4] / s[0] - w2 / 6.0;
-    d.e_r = s[5] / s[0] - w2 / 6.0;
-    d.pe = (P.gamma_e - 1.0) * (s[3] - s[0] * w2 / 6.0);
-    d.pi = (P.gamma_i - 1.0) * (s[4] - s[0] * w2 / 6.0);
-    d.pr = (P.gamma_r - 1.0) * (s[5] - s[0] * w2 / 6.0);
+    const double w6 = div6_rn(w2), rw6 = div6_rn(s[0] * w2);
+    d.e_e = div_rn(s[3], r0) - w6;
+    d.e_i = div_rn(s[4], r0) - w6;
+    d.e_r = div_rn(s[5], r0) - w6;
+    d.pe = (P.gamma_e - 1.0) * (s[3] - rw6);
+    d.pi = (P.gamma_i - 1.0) * (s[4] - rw6);
+    d.pr = (P.gamma_r - 1.0) * (s[5] - rw6);
     return d;
 }
 
 // state.rs:245-276 te, ti, tr (diffusion and source only)
 __device__ __forceinline__ void temps_from_state(const double s[6], const DevParams& P, double& te, double& ti,
                                                  double& tr) {
-    double u = s[1] / s[0], v = s[2] / s[0];
+    const Recip r0 = recip(s[0]);
+    double u = div_rn(s[1], r0), v = div_rn(s[2], r0);
     double w2 = sqd(u) + sqd(v);
     te = s[3] / (s[0] * P.cve) - w2 / (6.0 * P.cve);
     ti = s[4] / (s[0] * P.cvi) - w2 / (6.0 * P.cvi);
-    double er_term = s[5] / s[0] - w2 / 6.0;
+    double er_term = div_rn(s[5], r0) - div6_rn(w2);
     tr = cr_pow_quarter(er_term * s[0] / P.a_rad);
 }
 
@@ -128,12 +141,13 @@ __device__ __forceinline__ Roe roe_average(double rho_s1, const Prim& d3, double
     Roe q;
     double rho1 = sqrt(rho_s1), rho2 = sqrt(rho_s2);
     double rho_sum = rho1 + rho2;
-    q.u = (d3.u * rho1 + d2.u * rho2) / rho_sum;
-    q.v = (d3.v * rho1 + d2.v * rho2) / rho_sum;
+    const Recip rs = recip(rho_sum);
+    q.u = div_rn(d3.u * rho1 + d2.u * rho2, rs);
+    q.v = div_rn(d3.v * rho1 + d2.v * rho2, rs);
     q.w2 = sqd(q.u) + sqd(q.v);
-    q.ee = (d3.e_e * rho1 + d2.e_e * rho2) / rho_sum;
-    q.ei = (d3.e_i * rho1 + d2.e_i * rho2) / rho_sum;
-    q.er = (d3.e_r * rho1 + d2.e_r * rho2) / rho_sum;
+    q.ee = div_rn(d3.e_e * rho1 + d2.e_e * rho2, rs);
+    q.ei = div_rn(d3.e_i * rho1 + d2.e_i * rho2, rs);
+    q.er = div_rn(d3.e_r * rho1 + d2.e_r * rho2, rs);
     const double GE = P.gamma_e, GI = P.gamma_i, GR = P.gamma_r;
     const double gi = GI - 1.0, ge = GE - 1.0, gr = GR - 1.0;
     const double gt = gi + ge + gr;
@@ -222,38 +236,38 @@ __device__ __forceinline__ void r_col(int col, const RoeT<T>& q, const DevParams
         switch (col) {
         case 0:
             R[0] = 1.0; R[1] = u - cs; R[2] = v;
-            R[3] = GE * q.ee + w2 / 6.0 - u * cs / 3.0;
-            R[4] = GI * q.ei + w2 / 6.0 - u * cs / 3.0;
-            R[5] = GR * q.er + w2 / 6.0 - u * cs / 3.0;
+            R[3] = GE * q.ee + quot6(w2) - quot3(u * cs);
+            R[4] = GI * q.ei + quot6(w2) - quot3(u * cs);
+            R[5] = GR * q.er + quot6(w2) - quot3(u * cs);
             lam = u - cs; break;
         case 1: R[0] = 1.0; R[1] = u; R[2] = v; R[3] = gt * w2 / (6.0 * ge); R[4] = gr; R[5] = -gi; lam = u; break;
         case 2: R[0] = 1.0; R[1] = u; R[2] = v; R[3] = -gr; R[4] = gt * w2 / (6.0 * gi); R[5] = ge; lam = u; break;
         case 3: R[0] = 1.0; R[1] = u; R[2] = v; R[3] = gi; R[4] = -ge; R[5] = gt * w2 / (6.0 * gr); lam = u; break;
-        case 4: R[0] = 0.0; R[1] = 0.0; R[2] = 1.0; R[3] = v / 3.0; R[4] = v / 3.0; R[5] = v / 3.0; lam = u; break;
+        case 4: R[0] = 0.0; R[1] = 0.0; R[2] = 1.0; R[3] = quot3(v); R[4] = quot3(v); R[5] = quot3(v); lam = u; break;
         default:
             R[0] = 1.0; R[1] = u + cs; R[2] = v;
-            R[3] = GE * q.ee + w2 / 6.0 + u * cs / 3.0;
-            R[4] = GI * q.ei + w2 / 6.0 + u * cs / 3.0;
-            R[5] = GR * q.er + w2 / 6.0 + u * cs / 3.0;
+            R[3] = GE * q.ee + quot6(w2) + quot3(u * cs);
+            R[4] = GI * q.ei + quot6(w2) + quot3(u * cs);
+            R[5] = GR * q.er + quot6(w2) + quot3(u * cs);
             lam = u + cs; break;
         }
     } else {
         switch (col) {
         case 0:
             R[0] = 1.0; R[1] = u; R[2] = v - cs;
-            R[3] = GE * q.ee + w2 / 6.0 - v * cs / 3.0;
-            R[4] = GI * q.ei + w2 / 6.0 - v * cs / 3.0;
-            R[5] = GR * q.er + w2 / 6.0 - v * cs / 3.0;
+            R[3] = GE * q.ee + quot6(w2) - quot3(v * cs);
+            R[4] = GI * q.ei + quot6(w2) - quot3(v * cs);
+            R[5] = GR * q.er + quot6(w2) - quot3(v * cs);
             lam = v - cs; break;
-        case 1: R[0] = 0.0; R[1] = 1.0; R[2] = 0.0; R[3] = u / 3.0; R[4] = u / 3.0; R[5] = u / 3.0; lam = v; break;
+        case 1: R[0] = 0.0; R[1] = 1.0; R[2] = 0.0; R[3] = quot3(u); R[4] = quot3(u); R[5] = quot3(u); lam = v; break;
         case 2: R[0] = 1.0; R[1] = u; R[2] = v; R[3] = gt * w2 / (6.0 * ge); R[4] = gr; R[5] = -gi; lam = v; break;
         case 3: R[0] = 1.0; R[1] = u; R[2] = v; R[3] = -gr; R[4] = gt * w2 / (6.0 * gi); R[5] = ge; lam = v; break;
         case 4: R[0] = 1.0; R[1] = u; R[2] = v; R[3] = gi; R[4] = -ge; R[5] = gt * w2 / (6.0 * gr); lam = v; break;
         default:
             R[0] = 1.0; R[1] = u; R[2] = v + cs;
-            R[3] = GE * q.ee + w2 / 6.0 + v * cs / 3.0;
-            R[4] = GI * q.ei + w2 / 6.0 + v * cs / 3.0;
-            R[5] = GR * q.er + w2 / 6.0 + v * cs / 3.0;
+            R[3] = GE * q.ee + quot6(w2) + quot3(v * cs);
+            R[4] = GI * q.ei + quot6(w2) + quot3(v * cs);
+            R[5] = GR * q.er + quot6(w2) + quot3(v * cs);
             lam = v + cs; break;
         }
     }
@@ -275,14 +289,14 @@ __device__ __forceinline__ void r_row(int row, const Roe& q, const DevParams& P,
         case 1: R[0] = u - cs; R[1] = u; R[2] = u; R[3] = u; R[4] = 0.0; R[5] = u + cs; break;
         case 2: R[0] = v; R[1] = v; R[2] = v; R[3] = v; R[4] = 1.0; R[5] = v; break;
         case 3:
-            R[0] = GE * q.ee + w2 / 6.0 - u * cs / 3.0; R[1] = gt * w2 / (6.0 * ge); R[2] = -gr; R[3] = gi;
-            R[4] = v / 3.0; R[5] = GE * q.ee + w2 / 6.0 + u * cs / 3.0; break;
+            R[0] = GE * q.ee + div6_rn(w2) - div3_rn(u * cs); R[1] = gt * w2 / (6.0 * ge); R[2] = -gr; R[3] = gi;
+            R[4] = div3_rn(v); R[5] = GE * q.ee + div6_rn(w2) + div3_rn(u * cs); break;
         case 4:
-            R[0] = GI * q.ei + w2 / 6.0 - u * cs / 3.0; R[1] = gr; R[2] = gt * w2 / (6.0 * gi); R[3] = -ge;
-            R[4] = v / 3.0; R[5] = GI * q.ei + w2 / 6.0 + u * cs / 3.0; break;
+            R[0] = GI * q.ei + div6_rn(w2) - div3_rn(u * cs); R[1] = gr; R[2] = gt * w2 / (6.0 * gi); R[3] = -ge;
+            R[4] = div3_rn(v); R[5] = GI * q.ei + div6_rn(w2) + div3_rn(u * cs); break;
         default:
-            R[0] = GR * q.er + w2 / 6.0 - u * cs / 3.0; R[1] = -gi; R[2] = ge; R[3] = gt * w2 / (6.0 * gr);
-            R[4] = v / 3.0; R[5] = GR * q.er + w2 / 6.0 + u * cs / 3.0; break;
+            R[0] = GR * q.er + div6_rn(w2) - div3_rn(u * cs); R[1] = -gi; R[2] = ge; R[3] = gt * w2 / (6.0 * gr);
+            R[4] = div3_rn(v); R[5] = GR * q.er + div6_rn(w2) + div3_rn(u * cs); break;
         }
     } else {
         switch (row) {
@@ -290,14 +304,87 @@ __device__ __forceinline__ void r_row(int row, const Roe& q, const DevParams& P,
         case 1: R[0] = u; R[1] = 1.0; R[2] = u; R[3] = u; R[4] = u; R[5] = u; break;
         case 2: R[0] = v - cs; R[1] = 0.0; R[2] = v; R[3] = v; R[4] = v; R[5] = v + cs; break;
         case 3:
-            R[0] = GE * q.ee + w2 / 6.0 - v * cs / 3.0; R[1] = u / 3.0; R[2] = gt * w2 / (6.0 * ge); R[3] = -gr;
-            R[4] = gi; R[5] = GE * q.ee + w2 / 6.0 + v * cs / 3.0; break;
+            R[0] = GE * q.ee + div6_rn(w2) - div3_rn(v * cs); R[1] = div3_rn(u); R[2] = gt * w2 / (6.0 * ge); R[3] = -gr;
+            R[4] = gi; R[5] = GE * q.ee + div6_rn(w2) + div3_rn(v * cs); break;
         case 4:
-            R[0] = GI * q.ei + w2 / 6.0 - v * cs / 3.0; R[1] = u / 3.0; R[2] = gr; R[3] = gt * w2 / (6.0 * gi);
-            R[4] = -ge; R[5] = GI * q.ei + w2 / 6.0 + v * cs / 3.0; break;
+            R[0] = GI * q.ei + div6_rn(w2) - div3_rn(v * cs); R[1] = div3_rn(u); R[2] = gr; R[3] = gt * w2 / (6.0 * gi);
+            R[4] = -ge; R[5] = GI * q.ei + div6_rn(w2) + div3_rn(v * cs); break;
         default:
-            R[0] = GR * q.er + w2 / 6.0 - v * cs / 3.0; R[1] = u / 3.0; R[2] = -gi; R[3] = ge;
-            R[4] = gt * w2 / (6.0 * gr); R[5] = GR * q.er + w2 / 6.0 + v * cs / 3.0; break;
+            R[0] = GR * q.er + div6_rn(w2) - div3_rn(v * cs); R[1] = div3_rn(u); R[2] = -gi; R[3] = ge;
+            R[4] = gt * w2 / (6.0 * gr); R[5] = GR * q.er + div6_rn(w2) + div3_rn(v * cs); break;
+        }
+    }
+}
+
+// The divisors of one face's left eigenvector rows (weno.rs:79-458):
+// 12 cs2, b, 6 cs2, 3 cs2, gt cs2 and gt, each with its reciprocal, formed
+// once per face and shared by the rows (divrn.cuh: every quotient is still
+// the IEEE one).
+struct RoeDiv {
+    Recip den, b, c6, c3, cg, gt;
+};
+__device__ __forceinline__ RoeDiv roe_div(const Roe& q, const DevParams& P) {
+    const double gt = (P.gamma_i - 1.0) + (P.gamma_e - 1.0) + (P.gamma_r - 1.0);
+    RoeDiv r;
+    r.den = recip(q.den);
+    r.b = recip(q.b);
+    r.c6 = recip(6.0 * q.cs2);
+    r.c3 = recip(3.0 * q.cs2);
+    r.cg = recip(gt * q.cs2);
+    r.gt = recip(gt);
+    return r;
+}
+
+// l_row over double with the face's shared divisors: the same expressions
+// as l_row<DIR, T> (weno.rs:79-458), the same roundings.
+template <int DIR>
+__device__ __forceinline__ void l_row(int row, const Roe& q, const RoeDiv& rd, const DevParams& P, double L[6]) {
+    const double GE = P.gamma_e, GI = P.gamma_i, GR = P.gamma_r;
+    const double gi = GI - 1.0, ge = GE - 1.0, gr = GR - 1.0;
+    const double gt = gi + ge + gr;
+    const double u = q.u, v = q.v, w2 = q.w2, cs = q.cs, cs2 = q.cs2;
+    int mode;
+    if (DIR == 0) {
+        const int m[6] = {0, 2, 3, 4, 1, 5};
+        mode = m[row];
+    } else {
+        mode = row;
+    }
+    if (mode == 0 || mode == 5) {
+        if (DIR == 0) {
+            L[0] = mode == 0 ? div_rn(gt * w2 + 6.0 * u * cs, rd.den) : div_rn(gt * w2 - 6.0 * u * cs, rd.den);
+            L[1] = mode == 0 ? div_rn(-2.0 * gt * u - 6.0 * cs, rd.den) : div_rn(-2.0 * gt * u + 6.0 * cs, rd.den);
+            L[2] = div_rn(-2.0 * gt * v, rd.den);
+        } else {
+            L[0] = mode == 0 ? div_rn(gt * w2 + 6.0 * v * cs, rd.den) : div_rn(gt * w2 - 6.0 * v * cs, rd.den);
+            L[1] = div_rn(-2.0 * gt * u, rd.den);
+            L[2] = mode == 0 ? div_rn(-2.0 * gt * v - 6.0 * cs, rd.den) : div_rn(-2.0 * gt * v + 6.0 * cs, rd.den);
+        }
+        L[3] = div_rn(6.0 * ge, rd.den);
+        L[4] = div_rn(6.0 * gi, rd.den);
+        L[5] = div_rn(6.0 * gr, rd.den);
+    } else if (mode == 1) {
+        if (DIR == 0) { L[0] = -v; L[1] = 0.0; L[2] = 1.0; }
+        else { L[0] = -u; L[1] = 1.0; L[2] = 0.0; }
+        L[3] = 0.0; L[4] = 0.0; L[5] = 0.0;
+    } else {
+        const double gk = mode == 2 ? ge : (mode == 3 ? gi : gr);
+        const double hk = mode == 2 ? q.he : (mode == 3 ? q.hi : q.hr);
+        L[0] = div_rn(gk, rd.gt) - div_rn(gk * w2, rd.c6) - div_rn(gk * gt * w2, rd.b) * (hk - cs2 * w2);
+        L[1] = div_rn(gk * u, rd.c3) + div_rn(2.0 * gk * gt * u, rd.b) * (hk - cs2 * w2);
+        L[2] = div_rn(gk * v, rd.c3) + div_rn(2.0 * gk * gt * v, rd.b) * (hk - cs2 * w2);
+        if (mode == 2) {
+            L[3] = div_rn(-sqd(ge), rd.cg) - div_rn(6.0 * ge, rd.b) * (ge * hk - gt * cs2 * w2);
+            L[4] = div_rn(-ge * gi, rd.cg) - div_rn(6.0 * ge * gi, rd.b) * (hk - 6.0 * gr * cs2);
+            L[5] = div_rn(-ge * gr, rd.cg) - div_rn(6.0 * ge * gr, rd.b) * (hk + 6.0 * gi * cs2);
+        } else if (mode == 3) {
+            L[3] = div_rn(-gi * ge, rd.cg) - div_rn(6.0 * gi * ge, rd.b) * (hk + 6.0 * gr * cs2);
+            L[4] = div_rn(-sqd(gi), rd.cg) - div_rn(6.0 * gi, rd.b) * (gi * hk - gt * cs2 * w2);
+            L[5] = div_rn(-gi * gr, rd.cg) - div_rn(6.0 * gi * gr, rd.b) * (hk - 6.0 * ge * cs2);
+        } else {
+            L[3] = div_rn(-gr * ge, rd.cg) - div_rn(6.0 * gr * ge, rd.b) * (hk - 6.0 * gi * cs2);
+            L[4] = div_rn(-gr * gi, rd.cg) - div_rn(6.0 * gr * gi, rd.b) * (hk + 6.0 * ge * cs2);
+            L[5] = div_rn(-sqd(gr), rd.cg) - div_rn(6.0 * gr, rd.b) * (gr * hk - gt * cs2 * w2);
         }
     }
 }
@@ -436,10 +523,11 @@ __device__ __forceinline__ double weno5(double u0, double u1, double u2, double 
     double a1 = 0.6 / sqd(eps + beta1);
     double a2 = 0.3 / sqd(eps + beta2);
     double sum_o = a0 + a1 + a2;
-    double w0 = a0 / sum_o, w1 = a1 / sum_o, w2 = a2 / sum_o;
-    double p0 = u0 / 3.0 - 7.0 / 6.0 * u1 + 11.0 / 6.0 * u2;
-    double p1 = -u1 / 6.0 + 5.0 / 6.0 * u2 + u3 / 3.0;
-    double p2 = u2 / 3.0 + 5.0 / 6.0 * u3 - u4 / 6.0;
+    const Recip rs = recip(sum_o); // the three weights share their divisor (IEEE quotients, divrn.cuh)
+    double w0 = div_rn(a0, rs), w1 = div_rn(a1, rs), w2 = div_rn(a2, rs);
+    double p0 = div3_rn(u0) - 7.0 / 6.0 * u1 + 11.0 / 6.0 * u2;
+    double p1 = div6_rn(-u1) + 5.0 / 6.0 * u2 + div3_rn(u3);
+    double p2 = div3_rn(u2) + 5.0 / 6.0 * u3 - div6_rn(u4);
     return w0 * p0 + w1 * p1 + w2 * p2;
 }
 
@@ -487,6 +575,35 @@ __device__ __forceinline__ void noncon9(const double pe[9], const double pi[9], 
     out[0] = v / 3.0 * der_ee + (coef_left * jm_ee + coef_right * jp_ee) / ds;
     out[1] = v / 3.0 * der_ei + (coef_left * jm_ei + coef_right * jp_ei) / ds;
     out[2] = v / 3.0 * der_er + (coef_left * jm_er + coef_right * jp_er) / ds;
+}
+
+// noncon9 with the divisors 60 ds and ds given with their reciprocals (the
+// same quotients, divrn.cuh), for callers that hold them for many cells
+__device__ __forceinline__ void noncon9(const double pe[9], const double pi[9], const double pr[9],
+                                        const double vel[9], const Recip& r60ds, const Recip& rds, double out[3]) {
+    double v = vel[4];
+    auto d6r = [&](const double* q) {
+        return div_rn(q[7] - 9.0 * q[6] + 45.0 * q[5] - 45.0 * q[3] + 9.0 * q[2] - q[1], r60ds);
+    };
+    double dpe = d6r(pe), dpi = d6r(pi), dpr = d6r(pr);
+    double der_ee = 2.0 * dpe - dpi - dpr;
+    double der_ei = 2.0 * dpi - dpe - dpr;
+    double der_er = 2.0 * dpr - dpe - dpi;
+    double nee[9], nei[9], ner[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        nee[k] = 2.0 * pe[k] - pi[k] - pr[k];
+        nei[k] = 2.0 * pi[k] - pe[k] - pr[k];
+        ner[k] = 2.0 * pr[k] - pe[k] - pi[k];
+    }
+    double jm_ee = jump8(nee), jm_ei = jump8(nei), jm_er = jump8(ner);
+    double jp_ee = jump8(nee + 1), jp_ei = jump8(nei + 1), jp_er = jump8(ner + 1);
+    double coef_left = div3_rn(fmax(fmax(v, vel[3]), 0.0));
+    double coef_right = div3_rn(fmin(fmin(v, vel[5]), 0.0));
+    const double v3 = div3_rn(v);
+    out[0] = v3 * der_ee + div_rn(coef_left * jm_ee + coef_right * jp_ee, rds);
+    out[1] = v3 * der_ei + div_rn(coef_left * jm_ei + coef_right * jp_ei, rds);
+    out[2] = v3 * der_er + div_rn(coef_left * jm_er + coef_right * jp_er, rds);
 }
 
 // dt.rs:5-34 get_local_dt (same association order; CVE^3 = CVE*(CVE*CVE)),

@@ -25,7 +25,7 @@ constexpr bool kExactR = true;
 constexpr bool kExactR = false;
 #endif
 
-__global__ void __launch_bounds__(RHS_THREADS) k_rhs_stage(const Inst* __restrict__ insts, const Tile* __restrict__ tiles,
+__global__ void __launch_bounds__(RHS_THREADS, 2) k_rhs_stage(const Inst* __restrict__ insts, const Tile* __restrict__ tiles,
                                                    int nt, int stage, int mode, double* __restrict__ rhs_out) {
     __shared__ double sP[5][RHS_NPT]; // pe, pi, pr, u, v
     if (blockIdx.x >= nt) return;
@@ -73,14 +73,14 @@ __global__ void __launch_bounds__(RHS_THREADS) k_rhs_stage(const Inst* __restric
         const int p = hc + (q - 4) * HJ;
         pe[q] = sP[0][p]; pi[q] = sP[1][p]; pr[q] = sP[2][p]; vel[q] = sP[3][p];
     }
-    if (kExactR) noncon9(pe, pi, pr, vel, dx, ncx);
+    if (kExactR) noncon9(pe, pi, pr, vel, recip(60.0 * dx), recip(dx), ncx);
     else fastm::noncon9(pe, pi, pr, vel, 1.0 / (60.0 * dx), 1.0 / dx, ncx);
 #pragma unroll
     for (int q = 0; q < 9; ++q) {
         const int p = hc + (q - 4);
         pe[q] = sP[0][p]; pi[q] = sP[1][p]; pr[q] = sP[2][p]; vel[q] = sP[4][p];
     }
-    if (kExactR) noncon9(pe, pi, pr, vel, dy, ncy);
+    if (kExactR) noncon9(pe, pi, pr, vel, recip(60.0 * dy), recip(dy), ncy);
     else fastm::noncon9(pe, pi, pr, vel, 1.0 / (60.0 * dy), 1.0 / dy, ncy);
 #pragma unroll
     for (int k = 0; k < 3; ++k) rhs[3 + k] = rhs[3 + k] + ncx[k] + ncy[k];

@@ -11,11 +11,20 @@ workloads are the reference's Mach-3 half-cylinder at h = 1/320 (cyl961,
 961 x 3841 nodes), 1/160 and 1/40, and the planar shock. FP64 throughout.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                  [--workload batch256|cyl961|cyl481|cyl121|planar] [--exact]
+                  [--workload batch256|cyl961|cyl481|cyl121|planar] [--fma]
+
+The benched build is librh3t_exact: the reference's expressions and
+roundings (no FMA contraction, IEEE quotients, correctly rounded pow), the
+build whose results are checked against the oracle at <= 1e-10 (the line's
+`parity` object measures it on instances of the benched workload in the same
+run). --fma benches librh3t (FMA contraction, shared reciprocals; faster,
+its roundings differ from the reference's).
 
 --impl reference times the reference algorithm's CPU implementation (the
 oracle restatement, OpenMP on all host cores; the Rust reference cannot be
-built on this image) on the same workload and prints the same JSON line.
+built on this image) on the same workload and prints the same JSON line
+(same metric, config, steps and warm-up; each step a bounded sample of the
+workload, as its cpu_baseline.sample says).
 Multi-GPU runs are independent replicas (one instance per GPU, no exchange):
 value = all ranks' cell-updates / max-over-ranks device time.
 """
@@ -49,13 +58,13 @@ CFL = 0.05
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_flux
 # launch, from an ncu capture of `bench.py --steps 3 --warmup 3 --no-cpu
 # --no-e2e` (FMA build); None where no capture exists
-FLUX_TRAFFIC_BYTES = {"cyl961": 651.5e6}
+FLUX_TRAFFIC_BYTES = {"fma": {"cyl961": 651.5e6}, "exact": {}}
 # DRAM bytes per heavy ghost of one stage's ghost update (k_ghost_prep +
 # k_ghosts) and per active face of one k_flux launch, from ncu captures on
 # the batch24 workload (84,000 heavy ghosts, 1,714,456 faces), scaled by the
 # heavy-ghost and face counts of the batched workloads
-GHOST_TRAFFIC_PER_HEAVY = (902.88e6 + 7.24e6 + 15.32e6 + 9.25e6) / 84000
-FLUX_TRAFFIC_PER_FACE = (74.60e6 + 43.63e6) / 1714456
+GHOST_TRAFFIC_PER_HEAVY = {"fma": (902.88e6 + 7.24e6 + 15.32e6 + 9.25e6) / 84000, "exact": None}
+FLUX_TRAFFIC_PER_FACE = {"fma": (74.60e6 + 43.63e6) / 1714456, "exact": None}
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -202,25 +211,94 @@ def cpu_baseline(O, wl, budget_s=20.0, specs=None):
                       f"{el:.1f} s, after a {build_s:.1f} s ghost-grid build"}
 
 
+def rel_linf(a, b, mask):
+    """Normwise relative L-infinity deviation per field over fluid nodes
+    (max |a - b| / max |b|; both momentum components against the largest
+    momentum magnitude)."""
+    a, b = a[mask], b[mask]
+    scale = np.abs(b).max(0)
+    scale[1] = scale[2] = np.sqrt(b[:, 1] ** 2 + b[:, 2] ** 2).max()
+    scale[scale == 0] = 1.0
+    return np.abs(a - b).max(0) / scale
+
+
+def batch_config(spec, specs, cells, ghosts, heavy, world, state_mb):
+    """The `config` of a batch workload line: what defines the workload, the
+    same for the repo arm and the reference arm."""
+    classes = {}
+    for sp in specs:
+        classes[sp["nx"]] = classes.get(sp["nx"], 0) + 1
+    return {"workload": spec["name"], "instances": len(specs), "instances_by_nx": classes,
+            "scheme": "SSP-RK3, dt = 0.05 dt_cfl per step and instance", "fluid_cells": cells, "ghosts": ghosts,
+            "heavy_ghosts": heavy, "parallelism": "replicas" if world > 1 else "single",
+            "l2": "inputs larger than L2 (state buffers 3 x %.0f MB)" % state_mb}
+
+
 def run_reference(args):
+    """The reference arm: the oracle (the reference algorithm restated in
+    C++, OpenMP on all host threads) on the same workload, metric, config,
+    step and warm-up counts. A step advances a bounded, rotating sample of
+    the instances by one SSP-RK3 step each, sized so the whole run stays
+    within about two minutes; the metric (cell-updates/s) is a rate."""
     from oracle import oracle as O
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     spec = WORKLOADS[args.workload]
     threads = O.max_threads()
+    import importlib
+    rh = importlib.import_module("3t_rh_b200")
     if spec["kind"] == "batch":
-        import importlib
-        rh = importlib.import_module("3t_rh_b200")
         specs = rh.cases.batch_specs(spec["n"])
-        v, n_inst, steps, el, _ = batch_oracle_rate(O, specs, 60.0, max_steps=args.steps)
+        t0 = time.perf_counter()
+        cases = [oracle_batch_case(O, sp) for sp in specs]
+        build_s = time.perf_counter() - t0
+        cells = [int(c.fluid().sum()) for c in cases]
+        ghosts = sum(c.n_ghosts() for c in cases)
+        heavy = sum(c.n_heavy() for c in cases)
+        state_mb = 6 * 8 * sum((c.nx + 8) * (c.ny + 8) for c in cases) / 1e6
+        total = sum(cells)
+        # a short probe of one step per instance sizes the per-step sample
+        t0 = time.perf_counter()
+        probe = 0
+        for c, n in zip(cases, cells):
+            c.run(1, CFL)
+            probe += n
+            if time.perf_counter() - t0 > 2.0:
+                break
+        rate0 = probe / (time.perf_counter() - t0)
+        budget = 120.0
+        frac = min(1.0, budget * rate0 / (total * max(1, args.steps + args.warmup)))
+        per_step = max(1, int(round(frac * total)))
+        pos = [0]
+
+        def step():
+            done = 0
+            while done < per_step:
+                k = pos[0] % len(cases)
+                cases[k].run(1, CFL)
+                done += cells[k]
+                pos[0] += 1
+            return done
+
+        for _ in range(args.warmup):
+            step()
+        t0 = time.perf_counter()
+        done = 0
+        for _ in range(args.steps):
+            done += step()
+        el = time.perf_counter() - t0
+        v = done / el
         line = {"metric": "cell-updates/s", "value": v, "unit": "cell-updates/s", "n_gpus": args.gpus,
-                "steps": steps, "warmup": 0, "ms_per_step": 1e3 * el / steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-                "config": {"workload": spec["name"], "instances_timed": n_inst},
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "impl": "reference",
+                "config": batch_config(spec, specs, total, ghosts, heavy, args.gpus, state_mb),
                 "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": threads, "kind": "port",
-                                 "sample": f"{steps} SSP-RK3 step(s) of each of the first {n_inst} instances "
-                                           f"(bounded at ~60 s of stepping)"},
+                                 "sample": f"each step advances the next instances of the {len(specs)} in turn by one "
+                                           f"SSP-RK3 step until {per_step} fluid cells ({100 * per_step / total:.1f}% "
+                                           f"of the workload's {total}) are advanced; {args.steps} timed steps, "
+                                           f"{el:.1f} s; ghost-grid build {build_s:.1f} s not timed"},
                 "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return
@@ -247,6 +325,85 @@ def run_reference(args):
                              "sample": f"{steps} of {args.steps} requested SSP-RK3 steps (capped at ~120 s)"},
             "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+PARITY_SIZES = (61, 91, 121)
+
+
+def parity_instances(rh, per_size=3):
+    """The first `per_size` instances of each grid size of the batch256 workload."""
+    specs_all = rh.cases.batch_specs(256)
+    idx = []
+    for nx in PARITY_SIZES:
+        idx += [k for k, sp in enumerate(specs_all) if sp["nx"] == nx][:per_size]
+    return idx, [specs_all[k] for k in idx]
+
+
+def parity_record(rh, O, local, exact, steps=200, per_size=3):
+    """The benched build against the oracle on instances of the batch256
+    workload, advanced together for `steps` steps, each compared with the
+    oracle (glibc pow, the reference's libm) and with the oracle built with
+    the correctly rounded power the CUDA path computes. crpow_vs_oracle is
+    how far that last-bit change of libm alone moves the reference
+    algorithm."""
+    idx, specs = parity_instances(rh, per_size)
+    fields = [rh.cases.batch_field(sp) for sp in specs]
+    grids = rh.GhostGrid.build_many(fields, device=local)
+    b = rh.Batch(fields, grids, device=local, exact=exact)
+    b.advance(steps, CFL)
+    res = b.download()
+    b.close()
+    OC = O.crpow_variant()
+    per = []
+    t0 = time.perf_counter()
+    for k, sp, f, (u, _) in zip(idx, specs, fields, res):
+        ref, refc = oracle_batch_case(O, sp), oracle_batch_case(OC, sp)
+        ref.run(steps, CFL)
+        refc.run(steps, CFL)
+        r, rc = ref.state(), refc.state()
+        fl = f.fluid
+        per.append({"instance": k, "nx": sp["nx"], "mach": round(sp["mach"], 4),
+                    "vs_oracle": float(rel_linf(u, r, fl).max()),
+                    "vs_oracle_crpow": float(rel_linf(u, rc, fl).max()),
+                    "bitwise_vs_oracle_crpow": bool(np.array_equal(u[fl], rc[fl])),
+                    "crpow_vs_oracle": float(rel_linf(rc, r, fl).max())})
+    return {"build": "no FMA contraction" if exact else "FMA contraction", "steps": steps,
+            "instances_checked": len(per), "tolerance": 1e-10,
+            "max_rel_linf_vs_oracle": max(p["vs_oracle"] for p in per),
+            "max_rel_linf_vs_oracle_crpow": max(p["vs_oracle_crpow"] for p in per),
+            "all_bitwise_vs_oracle_crpow": all(p["bitwise_vs_oracle_crpow"] for p in per),
+            "max_crpow_vs_oracle": max(p["crpow_vs_oracle"] for p in per),
+            "metric": "max over fields of max|gpu - oracle| / max|oracle| over fluid nodes",
+            "oracle_s": round(time.perf_counter() - t0, 1), "per_instance": per}
+
+
+def scale_record(rh, torch, flops, local, exact, wl="cyl961", steps=20):
+    """The plain solver on one large instance (the reference's half-cylinder
+    at h = 1/320, 961 x 3841 nodes), the benched build: cell-updates/s over
+    `steps` graph-replayed steps and the flux kernel's FP64 rate."""
+    f = make_field(rh, wl)
+    g = rh.GhostGrid.build_many([f], device=local)[0]
+    s = rh.Solver(f, g, device=local, exact=exact)
+    cells = int(f.fluid.sum())
+    st = torch.cuda.ExternalStream(s.stream, device=torch.device(f"cuda:{local}"))
+    s.advance(3, CFL)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    s.advance(steps, CFL)
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    prof = s.profile_steps(5, CFL)
+    nxf, nyf = flops.face_counts(f.fluid, f.grid.nx, f.grid.ny)
+    fl_launch = flops.flux_launch_flops(nxf, nyf, False)
+    flux_ms, flux_n = prof["flux"]
+    total = sum(v[0] for v in prof.values())
+    s.close()
+    return {"workload": WORKLOADS[wl]["name"], "fluid_cells": cells, "steps": steps, "ms_per_step": ms / steps,
+            "value": cells * steps / (ms * 1e-3), "unit": "cell-updates/s",
+            "flux_tflops": fl_launch / (flux_ms / flux_n * 1e-3) / 1e12,
+            "kernel_share": {k: v[0] / total for k, v in prof.items()}}
 
 
 def adjoint_bench(rh, torch, local, exact, nsteps=200, ckpt=20, n=32):
@@ -383,15 +540,15 @@ def run_batch(args, rh, flops, torch, dist, world, rank, local):
     g_bytes = flops.ghost_launch_bytes(n_heavy)
     hbm, hbm_src = hbm_peak()
     g_achieved = g_bytes / (ghost_stage_ms * 1e-3) / 1e9
+    bkey = "exact" if args.exact else "fma"
     rl_flux = {"bound": "fp64", "kernel": "k_flux (x+y interface WENO5 fluxes, all instances)",
                "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-               "traffic": None if args.exact else FLUX_TRAFFIC_PER_FACE * n_faces,
+               "traffic": None if FLUX_TRAFFIC_PER_FACE[bkey] is None else FLUX_TRAFFIC_PER_FACE[bkey] * n_faces,
                "traffic_unit": "bytes per launch", "peak_source": "measured DFMA loop on this GPU (rh3t_fp64_peak)",
                "flops_per_launch": fl_launch, "launch_ms": flux_ms / flux_n}
     rl_ghost = {"bound": "hbm", "kernel": "k_ghost_prep + k_ghosts (one stage's ghost update, all instances)",
                 "achieved": g_achieved, "peak": hbm, "unit": "GB/s", "frac": g_achieved / hbm,
-                "traffic": None if GHOST_TRAFFIC_PER_HEAVY is None or args.exact
-                else GHOST_TRAFFIC_PER_HEAVY * n_heavy,
+                "traffic": None if GHOST_TRAFFIC_PER_HEAVY[bkey] is None else GHOST_TRAFFIC_PER_HEAVY[bkey] * n_heavy,
                 "traffic_unit": "bytes per stage", "peak_source": hbm_src,
                 "bytes_per_launch": g_bytes, "launch_ms": ghost_stage_ms,
                 "bytes_model": f"{flops.HEAVY_GHOST_BYTES} B of GhostBC tables per heavy ghost x {n_heavy}"}
@@ -444,30 +601,31 @@ def run_batch(args, rh, flops, torch, dist, world, rank, local):
         adj = adjoint_bench(rh, torch, local, args.exact, nsteps=args.adjoint_steps,
                             ckpt=min(20, args.adjoint_steps), n=args.adjoint_instances)
 
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
-        from oracle import oracle as O  # timed CPU baseline only
-        cpu = cpu_baseline(O, args.workload, specs=specs)
+    cpu = parity = scale = None
+    if rank == 0 and world == 1:
+        from oracle import oracle as O  # timed CPU baseline and parity reference only
+        if not args.no_cpu:
+            cpu = cpu_baseline(O, args.workload, specs=specs)
+        if not args.no_parity:
+            parity = parity_record(rh, O, local, args.exact, steps=args.parity_steps)
+    if rank == 0 and world == 1 and not args.no_scale:
+        scale = scale_record(rh, torch, flops, local, args.exact)
 
     if rank == 0:
-        classes = {}
-        for sp in specs:
-            classes[sp["nx"]] = classes.get(sp["nx"], 0) + 1
+        state_mb = 6 * 8 * sum((f.grid.nx + 8) * (f.grid.ny + 8) for f in fields) / 1e6
         line = {
             "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": spec["name"], "instances": b.n, "instances_by_nx": classes,
-                       "scheme": "SSP-RK3, dt = 0.05 dt_cfl per step and instance", "fluid_cells": cells,
-                       "ghosts": int(sum(g.len() for g in grids)),
-                       "heavy_ghosts": int(sum(g.n_heavy() for g in grids)),
-                       "parallelism": "replicas" if world > 1 else "single",
-                       "l2": "inputs larger than L2 (state buffers 3 x %.0f MB)" % (
-                           6 * 8 * sum((f.grid.nx + 8) * (f.grid.ny + 8) for f in fields) / 1e6),
-                       "arithmetic": "no FMA contraction" if args.exact else "FMA contraction",
-                       "ghost_build_s": round(build_s, 3), "ghost_build": "rh3t_geom_build_ghosts_device",
-                       "field_setup_s": round(fields_s, 3),
-                       "tile_shapes": {f"{e['nx']}x{e['ny']}": e["shape"] for e in tune}},
+            "config": batch_config(spec, specs, cells, int(sum(g.len() for g in grids)),
+                                   int(sum(g.n_heavy() for g in grids)), world, state_mb),
+            "arithmetic": "no FMA contraction, IEEE quotients, correctly rounded pow (the reference's "
+                          "roundings)" if args.exact else "FMA contraction, shared reciprocals",
+            "setup": {"ghost_build_s": round(build_s, 3), "ghost_build": "rh3t_geom_build_ghosts_device",
+                      "field_setup_s": round(fields_s, 3),
+                      "tile_shapes": {f"{e['nx']}x{e['ny']}": e["shape"] for e in tune}},
+            "parity": parity,
+            "plain_at_scale": scale,
             "instances_per_s": value / cells * b.n,
             "plain_one_at_a_time": None if plain_value is None else {
                 "value": plain_value, "unit": "cell-updates/s", "steps_per_instance": k_plain,
@@ -490,7 +648,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="batch256", choices=sorted(WORKLOADS))
-    ap.add_argument("--exact", action="store_true", help="bench the no-FMA-contraction build")
+    ap.add_argument("--fma", action="store_true", help="bench the FMA-contraction build (librh3t)")
+    ap.add_argument("--no-parity", action="store_true", help="skip the oracle parity record")
+    ap.add_argument("--parity-steps", type=int, default=200)
+    ap.add_argument("--no-scale", action="store_true", help="skip the 961x3841 plain-solver record")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--e2e-groups", type=int, default=8, help="instance groups of the pipelined host step")
@@ -499,6 +660,7 @@ def main():
     ap.add_argument("--adjoint-steps", type=int, default=200)
     ap.add_argument("--adjoint-instances", type=int, default=32)
     args = ap.parse_args()
+    args.exact = not args.fma
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return run_reference(args)
@@ -598,11 +760,12 @@ def main():
                        "parallelism": "replicas" if world > 1 else "single",
                        "l2": "inputs larger than L2 (state buffers 3 x %.0f MB)" % (
                            6 * 8 * (f.grid.nx + 8) * (f.grid.ny + 8) / 1e6),
-                       "arithmetic": "no FMA contraction" if args.exact else "FMA contraction",
                        "ghost_build_s": round(build_s, 3)},
+            "arithmetic": "no FMA contraction, IEEE quotients, correctly rounded pow (the reference's "
+                          "roundings)" if args.exact else "FMA contraction, shared reciprocals",
             "roofline": {"bound": "fp64", "kernel": "k_flux (x+y interface WENO5 fluxes)", "achieved": achieved,
                          "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                         "traffic": None if args.exact else FLUX_TRAFFIC_BYTES.get(args.workload),
+                         "traffic": FLUX_TRAFFIC_BYTES["exact" if args.exact else "fma"].get(args.workload),
                          "traffic_unit": "bytes per launch",
                          "peak_source": "measured DFMA loop on this GPU (rh3t_fp64_peak)",
                          "flops_per_launch": fl_launch, "launch_ms": flux_ms / flux_n,

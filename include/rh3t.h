@@ -375,6 +375,16 @@ int rh3t_fp64_peak(int32_t device, double* tflops);
  * out[3k+2] = x[k]^q. */
 int rh3t_math_check(int32_t device, const double* x, int32_t n, double q, double* out);
 
+/* Diagnostic (no reference counterpart): the shared-reciprocal divisions
+ * the solver uses in place of IEEE division where one divisor serves several
+ * quotients (Markstein's correction step from y = RN(1/b); the constants 3
+ * and 6) against the IEEE quotient, bit for bit, on n device-generated
+ * operand pairs: counts[0..5] the mismatches per category (0 random,
+ * 1 divisors with all-ones significands, 2 quotients next to a rounding
+ * midpoint, 3 range edges and special values, 4 a / 3, 5 a / 6);
+ * first[3] = a, b and the routine's quotient of one mismatch. */
+int rh3t_div_check(int32_t device, int64_t n, uint64_t seed, int64_t* counts, double* first);
+
 /* Diagnostic (no reference counterpart): the bounded mbarrier wait of the
  * ghost update (2^18 try_wait rounds, about a second on a B200, then
  * RH3T_ERR_DEVICE_TIMEOUT) run by

@@ -26,3 +26,20 @@ def test_correctly_rounded_powers(rh):
         bad_10 += out[k, 1] != float(m ** 10)
     assert bad_q == 0 and bad_10 == 0, (bad_q, bad_10)
     assert np.array_equal(out[:, 1], out[:, 2])
+
+
+def test_shared_reciprocal_division_bitwise(rh):
+    """Where one divisor serves several quotients, and for the constants 3
+    and 6, the solver divides by a shared reciprocal (Markstein's correction
+    step, csrc/divrn.cuh): every quotient must equal the IEEE one bit for
+    bit. 4e9 device-generated pairs: random operands over the fast path's
+    exponent range and beyond it, divisors with all-ones significands,
+    quotients next to a rounding midpoint, special values, and the two
+    constants."""
+    for exact in (True, False):
+        L = rh.load(exact)
+        counts = np.zeros(6, np.int64)
+        first = np.zeros(3)
+        seed = 1 if exact else 2
+        assert L.rh3t_div_check(0, 2_000_000_000, seed, counts.ctypes.data, first.ctypes.data) == 0
+        assert counts.sum() == 0, (counts.tolist(), first.tolist())
