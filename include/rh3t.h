@@ -334,7 +334,9 @@ int rh3t_calc_global_dt(rh3t_ctx* ctx, double* dt_cfl);
  * that every GPU loading the library keeps until exit: grids of more than
  * RH3T_DT_NOALLOC_MAX_CELLS nodes are rejected with
  * RH3T_ERR_INVALID_ARGUMENT. The first call on a device looks the array's
- * address up (cudaGetSymbolAddress): make it before any stream capture. All
+ * address up (cudaGetSymbolAddress) and keeps it for the life of the
+ * process, so the entry point must not be used on a device after a
+ * cudaDeviceReset of it: make the first call before any stream capture. All
  * calls share the array, so calls that overlap on the GPU race; calls
  * ordered on one stream are safe (each writes every entry it reads). */
 #define RH3T_DT_NOALLOC_MAX_CELLS (65536 * 256)

@@ -21,7 +21,7 @@ def test_noalloc_dt_matches_existing_entry_point_twice(rh):
     f = rh.cases.init_cylinder()
     g = rh.GhostGrid.build(f)
     s = rh.Solver(f, g)
-    L = rh.load()
+    L = s.L  # the same build as the solver the expected value comes from
     grid, prm = f.grid.to_c(), f.params.to_c()
     fluid_d = torch.tensor(f.fluid.astype(np.uint8), device="cuda")
     out_d = torch.zeros(1, dtype=torch.float64, device="cuda")
