@@ -4,9 +4,10 @@
 // A block of 6 warps covers 64 faces (a TI x TJ tile, shape chosen per tile)
 // in three phases:
 //   1. staging: the tile's stencil points (x faces: (TI + 5) x TJ points,
-//      y faces: TI x (TJ + 5)) with their physical flux go to shared memory
-//      once (the reference evaluates them once per face, six times per
-//      point), and each face's Roe state and activity flag are formed once;
+//      y faces: TI x (TJ + 5)) with their primitives and physical flux go to
+//      shared memory once (the reference evaluates them once per face, six
+//      times per point); then each face's Roe state, from the staged
+//      primitives of its points 3 and 2, and its activity flag;
 //   2. characteristic pass: warp c owns characteristic field c for the 64
 //      faces (two per lane), so the row of L, the projections and the two
 //      WENO5 reconstructions of f+ and f- are warp-uniform code; g_c goes to
@@ -45,6 +46,7 @@ struct FluxShared {
     double2 U[3][FLUX_NPT]; // (rho, mx), (my, ee), (ei, er)
     double2 F[3][FLUX_NPT];
     double T[3][FLUX_NPT];
+    double PR[5][FLUX_NPT]; // u, v, e_e, e_i, e_r of each point (the face Roe averages reuse them)
     double Q[NQ][FLUX_FACES];
     double G[6][FLUX_FACES];
     int act[FLUX_FACES];
@@ -148,66 +150,67 @@ __device__ __forceinline__ void flux_tile(const Inst& I, const Tile& t, int stag
     const int cols = 1 << t.lg, rows = FLUX_FACES >> t.lg;
     const int np = DIR == 0 ? (rows + 5) * cols : rows * (cols + 5);
     const bool diff = I.diffusion != 0;
-    // ---- 1. staging
-    for (int w = threadIdx.x; w < np + FLUX_FACES; w += blockDim.x) {
-        if (w < np) {
-            const int p = w;
-            int pi, pj;
-            if (DIR == 0) { pi = t.i - 3 + (p >> t.lg); pj = t.j0 + (p & (cols - 1)); }
-            else { const int r = p / (cols + 5); pi = t.i + r; pj = t.j0 - 3 + (p - r * (cols + 5)); }
-            double s[6] = {1.0, 0.0, 0.0, 1.0, 1.0, 1.0};
-            if (pi >= -RH3T_PAD && pi < nx + RH3T_PAD && pj >= -RH3T_PAD && pj < ny + RH3T_PAD)
-                load6(buf, plane, node_of(I, pi, pj), s);
-            Prim d = kExact ? prim_from_state(s, P) : fastm::prim(s, P);
-            double f[6];
-            phys_flux<DIR>(s, d, f);
+    // ---- 1. staging: points (state, primitives, physical flux), then faces
+    for (int p = threadIdx.x; p < np; p += blockDim.x) {
+        int pi, pj;
+        if (DIR == 0) { pi = t.i - 3 + (p >> t.lg); pj = t.j0 + (p & (cols - 1)); }
+        else { const int r = p / (cols + 5); pi = t.i + r; pj = t.j0 - 3 + (p - r * (cols + 5)); }
+        double s[6] = {1.0, 0.0, 0.0, 1.0, 1.0, 1.0};
+        if (pi >= -RH3T_PAD && pi < nx + RH3T_PAD && pj >= -RH3T_PAD && pj < ny + RH3T_PAD)
+            load6(buf, plane, node_of(I, pi, pj), s);
+        Prim d = kExact ? prim_from_state(s, P) : fastm::prim(s, P);
+        double f[6];
+        phys_flux<DIR>(s, d, f);
 #pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                S.U[k][p] = make_double2(s[2 * k], s[2 * k + 1]);
-                S.F[k][p] = make_double2(f[2 * k], f[2 * k + 1]);
-            }
-            if (diff) {
-                double te, ti, tr;
-                temps_from_state(s, P, te, ti, tr);
-                S.T[0][p] = te; S.T[1][p] = ti; S.T[2][p] = tr;
-            }
-        } else {
-            const int f = w - np;
-            int i, j, p0, ps;
-            face_index<DIR>(t, f, i, j, p0, ps);
-            bool valid = DIR == 0 ? (i <= nx && j < ny) : (i < nx && j <= ny);
-            if (valid) {
-                const uint8_t m0 = I.mask[node_of(I, i, j)];
-                const uint8_t m1 = DIR == 0 ? I.mask[node_of(I, i - 1, j)] : I.mask[node_of(I, i, j - 1)];
-                valid = (m0 | m1) != 0;
-            }
-            S.act[f] = valid ? 1 : 0;
-            if (!valid) continue;
-            double s3[6], s2[6];
-            load6(buf, plane, node_of(I, i, j), s3);
-            load6(buf, plane, DIR == 0 ? node_of(I, i - 1, j) : node_of(I, i, j - 1), s2);
-            Roe q;
-            if (kExact) {
-                const Prim d3 = prim_from_state(s3, P), d2 = prim_from_state(s2, P);
-                q = roe_average(s3[0], d3, s2[0], d2, P);
-            } else {
-                const Prim d3 = fastm::prim(s3, P), d2 = fastm::prim(s2, P);
-                const double a6[6] = {sqrt(s3[0]), d3.u, d3.v, d3.e_e, d3.e_i, d3.e_r};
-                const double b6[6] = {sqrt(s2[0]), d2.u, d2.v, d2.e_e, d2.e_i, d2.e_r};
-                q = fastm::roe(a6, b6, P);
-            }
-            double qv[NQ] = {q.u, q.v, q.w2, q.ee, q.ei, q.er, q.cs2, q.cs, q.he, q.hi, q.hr, q.b, q.den,
-                             0.0, 0.0, 0.0, 0.0, 0.0};
-            if (kExact) {
-                const RoeDiv rd = roe_div(q, P);
-                qv[13] = rd.den.y; qv[14] = rd.b.y; qv[15] = rd.c6.y; qv[16] = rd.c3.y; qv[17] = rd.cg.y;
-            } else {
-                qv[13] = 1.0 / q.cs2;
-                qv[14] = 1.0 / q.b;
-            }
-#pragma unroll
-            for (int k = 0; k < NQ; ++k) S.Q[k][f] = qv[k];
+        for (int k = 0; k < 3; ++k) {
+            S.U[k][p] = make_double2(s[2 * k], s[2 * k + 1]);
+            S.F[k][p] = make_double2(f[2 * k], f[2 * k + 1]);
         }
+        S.PR[0][p] = d.u; S.PR[1][p] = d.v; S.PR[2][p] = d.e_e; S.PR[3][p] = d.e_i; S.PR[4][p] = d.e_r;
+        if (diff) {
+            double te, ti, tr;
+            temps_from_state(s, P, te, ti, tr);
+            S.T[0][p] = te; S.T[1][p] = ti; S.T[2][p] = tr;
+        }
+    }
+    __syncthreads();
+    for (int f = threadIdx.x; f < FLUX_FACES; f += blockDim.x) {
+        int i, j, p0, ps;
+        face_index<DIR>(t, f, i, j, p0, ps);
+        bool valid = DIR == 0 ? (i <= nx && j < ny) : (i < nx && j <= ny);
+        if (valid) {
+            const uint8_t m0 = I.mask[node_of(I, i, j)];
+            const uint8_t m1 = DIR == 0 ? I.mask[node_of(I, i - 1, j)] : I.mask[node_of(I, i, j - 1)];
+            valid = (m0 | m1) != 0;
+        }
+        S.act[f] = valid ? 1 : 0;
+        if (!valid) continue;
+        // points[3] and points[2] of the face: the staged states and primitives
+        // (the same functions of the same states as a fresh evaluation)
+        const int p3 = p0 + 3 * ps, p2 = p0 + 2 * ps;
+        Prim d3, d2;
+        d3.u = S.PR[0][p3]; d3.v = S.PR[1][p3]; d3.e_e = S.PR[2][p3]; d3.e_i = S.PR[3][p3]; d3.e_r = S.PR[4][p3];
+        d2.u = S.PR[0][p2]; d2.v = S.PR[1][p2]; d2.e_e = S.PR[2][p2]; d2.e_i = S.PR[3][p2]; d2.e_r = S.PR[4][p2];
+        const double rho3 = S.U[0][p3].x, rho2 = S.U[0][p2].x;
+        Roe q;
+        if (kExact) {
+            q = roe_average(rho3, d3, rho2, d2, P);
+        } else {
+            const double a6[6] = {sqrt(rho3), d3.u, d3.v, d3.e_e, d3.e_i, d3.e_r};
+            const double b6[6] = {sqrt(rho2), d2.u, d2.v, d2.e_e, d2.e_i, d2.e_r};
+            q = fastm::roe(a6, b6, P);
+        }
+        double qv[NQ] = {q.u, q.v, q.w2, q.ee, q.ei, q.er, q.cs2, q.cs, q.he, q.hi, q.hr, q.b, q.den,
+                         0.0, 0.0, 0.0, 0.0, 0.0};
+        if (kExact) {
+            const RoeDiv rd = roe_div(q, P);
+            qv[13] = rd.den.y; qv[14] = rd.b.y; qv[15] = rd.c6.y; qv[16] = rd.c3.y; qv[17] = rd.cg.y;
+        } else {
+            qv[13] = 1.0 / q.cs2;
+            qv[14] = 1.0 / q.b;
+        }
+#pragma unroll
+        for (int k = 0; k < NQ; ++k) S.Q[k][f] = qv[k];
     }
     __syncthreads();
     const int c = threadIdx.x >> 5, lane = threadIdx.x & 31; // warp-uniform characteristic field
