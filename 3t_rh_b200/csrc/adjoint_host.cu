@@ -121,9 +121,9 @@ void enqueue_recorded_step(rh3t_ctx* c, double* rec) {
     for (int st = 0; st < 3; ++st) {
         launch_ghosts(s, c->d_inst, c->d_gpart, nh, c->d_gpart + c->n_gheavy, nc, c->d_hrec, st);
         launch_adj_copy(s, c->d_inst, 0, c->n_inst, mp, st, rec + st * np, 0);
-        enqueue_flux(c, s, st, r);
+        const int nf = enqueue_flux(c, s, st, r);
         enqueue_rhs(c, s, st, 2, rec + (3 + st) * np, r);
-        c->launches += ghost_launches(nh, nc) + 3;
+        c->launches += ghost_launches(nh, nc) + nf + 2;
     }
     c->launches += 1;
 }

@@ -127,10 +127,12 @@ int make_tiles(rh3t_ctx* c) {
     return RH3T_OK;
 }
 
-void enqueue_flux(rh3t_ctx* c, cudaStream_t s, int stage, Span r) {
+// returns the number of kernels launched
+int enqueue_flux(rh3t_ctx* c, cudaStream_t s, int stage, Span r) {
     const HostInst &a = c->hi[r.k0], &b = c->hi[r.k1 - 1];
     const int ntx = b.tx0 + b.ntx - a.tx0, nty = b.ty0 + b.nty - a.ty0;
     launch_flux(s, c->d_inst, c->d_tx + a.tx0, ntx, c->d_ty + a.ty0, nty, stage);
+    return flux_launches(ntx, nty);
 }
 
 void enqueue_rhs(rh3t_ctx* c, cudaStream_t s, int stage, int mode, double* rhs, Span r) {
@@ -166,9 +168,9 @@ void enqueue_dt(rh3t_ctx* c, cudaStream_t s, int mode, Span r) {
 void enqueue_stage(rh3t_ctx* c, int stage, Span r) {
     cudaStream_t s = c->stream;
     const int ng = enqueue_ghosts(c, s, stage, r);
-    enqueue_flux(c, s, stage, r);
+    const int nf = enqueue_flux(c, s, stage, r);
     enqueue_rhs(c, s, stage, 1, nullptr, r);
-    c->launches += ng + 2;
+    c->launches += ng + nf + 1;
 }
 
 void enqueue_step(rh3t_ctx* c, Span r) {
@@ -180,7 +182,9 @@ void enqueue_step(rh3t_ctx* c, Span r) {
 long long launches_per_step(const rh3t_ctx* c) {
     int nh, nc;
     ghost_counts(c, all(c), nh, nc);
-    return 1 + 3 * (ghost_launches(nh, nc) + 2);
+    const HostInst &a = c->hi[0], &b = c->hi[c->n_inst - 1];
+    const int nf = flux_launches(b.tx0 + b.ntx - a.tx0, b.ty0 + b.nty - a.ty0);
+    return 1 + 3 * (ghost_launches(nh, nc) + nf + 1);
 }
 
 // bc1.rs:930-1037 / 471-545: nearest fluid node to the mirror point 2 P0 - Pg
@@ -492,11 +496,11 @@ int l_instance(rh3t_ctx* c, int k, double* rhs, double* ghost_values) {
     DevScalars* sc = c->d_sc + k;
     CK(c, cudaMemcpyAsync(&sc->t_stage[0], &sc->t_after, sizeof(double), cudaMemcpyDeviceToDevice, s));
     const int ng = enqueue_ghosts(c, s, 0, r);
-    enqueue_flux(c, s, 0, r);
+    const int nf = enqueue_flux(c, s, 0, r);
     double* planes = c->d_io2 + 6 * H.cell_off;
     CK(c, cudaMemsetAsync(planes, 0, (size_t)n * 6 * sizeof(double), s));
     enqueue_rhs(c, s, 0, 0, c->d_io2, r);
-    c->launches += ng + 2;
+    c->launches += ng + nf + 1;
     if (rhs) {
         double* aos = c->d_io + 6 * H.cell_off;
         launch_planes_to_aos(s, planes, n, aos);
@@ -972,8 +976,8 @@ extern "C" int rh3t_profile_steps(rh3t_ctx* c, int32_t nsteps, double cfl_factor
         for (int st = 0; st < 3; ++st) {
             const int ng = enqueue_ghosts(c, s, st, r);
             mark(0, ng);
-            enqueue_flux(c, s, st, r);
-            mark(1, 1);
+            const int nf = enqueue_flux(c, s, st, r);
+            mark(1, nf);
             enqueue_rhs(c, s, st, 1, nullptr, r);
             mark(2, 1);
         }

@@ -83,7 +83,8 @@ int make_tiles(rh3t_ctx* c);
 // x-face, y-face and RHS tiles of one instance for a given shape
 void instance_tiles(const HostInst& H, const Shape& sh, int inst, std::vector<Tile>* tx, std::vector<Tile>* ty,
                     std::vector<Tile>* tr);
-void enqueue_flux(rh3t_ctx* c, cudaStream_t s, int stage, Span r);
+// returns the number of kernels launched (x and y faces: flux_launches)
+int enqueue_flux(rh3t_ctx* c, cudaStream_t s, int stage, Span r);
 void enqueue_rhs(rh3t_ctx* c, cudaStream_t s, int stage, int mode, double* rhs, Span r);
 void adj_free(rh3t_ctx* c);
 void io_free(rh3t_ctx* c);

@@ -40,6 +40,11 @@ __device__ __forceinline__ bool div_in_range(double x) {
     return e - 0x30500000u <= 0x1f400000u; // biased exponent in [1023 - 250, 1023 + 250]
 }
 
+// the IEEE quotient, out of line: the rare operands outside the fast range
+// take it, and one copy of its code serves every call site (the callers'
+// code stays small enough for the instruction cache)
+static __device__ __noinline__ double div_ieee(double a, double b) { return __ddiv_rn(a, b); }
+
 struct Recip {
     double b, y;
     bool ok;
@@ -64,7 +69,7 @@ __device__ __forceinline__ Recip recip_of(double b, double y) {
 
 // a / d.b, correctly rounded
 __device__ __forceinline__ double div_rn(double a, const Recip& d) {
-    if (!(d.ok && div_in_range(a))) return __ddiv_rn(a, d.b);
+    if (!(d.ok && div_in_range(a))) return div_ieee(a, d.b);
     double q = __dmul_rn(a, d.y);
     double r = __fma_rn(-d.b, q, a);
     q = __fma_rn(r, d.y, q);
@@ -74,14 +79,14 @@ __device__ __forceinline__ double div_rn(double a, const Recip& d) {
 
 // a / 3.0 and a / 6.0, correctly rounded
 __device__ __forceinline__ double div3_rn(double a) {
-    if (!div_in_range(a)) return __ddiv_rn(a, 3.0);
+    if (!div_in_range(a)) return div_ieee(a, 3.0);
     const double y = 0x1.5555555555555p-2; // RN(1/3)
     const double q = __dmul_rn(a, y);
     const double r = __fma_rn(-3.0, q, a);
     return __fma_rn(r, y, q);
 }
 __device__ __forceinline__ double div6_rn(double a) {
-    if (!div_in_range(a)) return __ddiv_rn(a, 6.0);
+    if (!div_in_range(a)) return div_ieee(a, 6.0);
     const double y = 0x1.5555555555555p-3; // RN(1/6)
     const double q = __dmul_rn(a, y);
     const double r = __fma_rn(-6.0, q, a);

@@ -242,26 +242,23 @@ __device__ __forceinline__ void flux_tile(const Inst& I, const Tile& t, int stag
 #define FLUX_MIN_BLOCKS_EXACT 4
 #endif
 constexpr int FLUX_MIN_BLOCKS = kExact ? FLUX_MIN_BLOCKS_EXACT : 5;
-__global__ void __launch_bounds__(FLUX_THREADS, FLUX_MIN_BLOCKS) k_flux(const Inst* __restrict__ insts, const Tile* __restrict__ tx,
-                                                       int ntx, const Tile* __restrict__ ty, int nty, int stage) {
+// x faces and y faces in two launches: each kernel holds one direction's
+// code, half of what an instruction cache shared by both would need
+template <int DIR>
+__global__ void __launch_bounds__(FLUX_THREADS, FLUX_MIN_BLOCKS) k_flux(const Inst* __restrict__ insts,
+                                                                     const Tile* __restrict__ tiles, int stage) {
     __shared__ FluxShared S;
-    const int b = blockIdx.x;
-    if (b < ntx) {
-        const Tile t = tx[b];
-        const Inst& I = insts[t.inst];
-        if (has_error(I)) return;
-        flux_tile<0>(I, t, stage, S);
-    } else if (b < ntx + nty) {
-        const Tile t = ty[b - ntx];
-        const Inst& I = insts[t.inst];
-        if (has_error(I)) return;
-        flux_tile<1>(I, t, stage, S);
-    }
+    const Tile t = tiles[blockIdx.x];
+    const Inst& I = insts[t.inst];
+    if (has_error(I)) return;
+    flux_tile<DIR>(I, t, stage, S);
 }
 
 void launch_flux(cudaStream_t s, const Inst* insts, const Tile* tx, int ntx, const Tile* ty, int nty, int stage) {
-    if (ntx + nty <= 0) return;
-    k_flux<<<ntx + nty, FLUX_THREADS, 0, s>>>(insts, tx, ntx, ty, nty, stage);
+    if (ntx > 0) k_flux<0><<<ntx, FLUX_THREADS, 0, s>>>(insts, tx, stage);
+    if (nty > 0) k_flux<1><<<nty, FLUX_THREADS, 0, s>>>(insts, ty, stage);
 }
+
+int flux_launches(int ntx, int nty) { return (ntx > 0 ? 1 : 0) + (nty > 0 ? 1 : 0); }
 
 } // namespace rh3t

@@ -10,7 +10,9 @@ namespace rh3t {
 void launch_ghosts(cudaStream_t s, const Inst* insts, const GhostRec* heavy, int nh, const GhostRec* cheap, int nc,
                    double* hrec, int stage);
 int ghost_launches(int nh, int nc);
+// x faces, then y faces: flux_launches() kernels
 void launch_flux(cudaStream_t s, const Inst* insts, const Tile* tx, int ntx, const Tile* ty, int nty, int stage);
+int flux_launches(int ntx, int nty);
 void launch_rhs_stage(cudaStream_t s, const Inst* insts, const Tile* tc, int nt, int stage, int mode, double* rhs);
 void launch_dt(cudaStream_t s, const Inst* insts, const Tile* tc, int nt, int mode);
 void launch_set_dt(cudaStream_t s, const Inst* insts, int n_inst, double dt);

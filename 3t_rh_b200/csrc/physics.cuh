@@ -514,8 +514,9 @@ __device__ __forceinline__ double weno5(double u0, double u1, double u2, double 
 
 } // namespace fastm
 
-// weno.rs:847-886 weno5 (WENO-JS, p = 2)
-__device__ __forceinline__ double weno5(double u0, double u1, double u2, double u3, double u4, double eps) {
+// weno.rs:847-886 weno5 (WENO-JS, p = 2); out of line: a face's twelve
+// reconstructions share one copy of its code
+static __device__ __noinline__ double weno5(double u0, double u1, double u2, double u3, double u4, double eps) {
     double beta2 = 13.0 / 12.0 * sqd(u2 - 2.0 * u3 + u4) + 0.25 * sqd(3.0 * u2 - 4.0 * u3 + u4);
     double beta1 = 13.0 / 12.0 * sqd(u1 - 2.0 * u2 + u3) + 0.25 * sqd(u1 - u3);
     double beta0 = 13.0 / 12.0 * sqd(u0 - 2.0 * u1 + u2) + 0.25 * sqd(u0 - 4.0 * u1 + 3.0 * u2);

@@ -397,7 +397,7 @@ def scale_record(rh, torch, flops, local, exact, wl="cyl961", steps=20):
     prof = s.profile_steps(5, CFL)
     nxf, nyf = flops.face_counts(f.fluid, f.grid.nx, f.grid.ny)
     fl_launch = flops.flux_launch_flops(nxf, nyf, False)
-    flux_ms, flux_n = prof["flux"]
+    flux_ms, flux_n = prof["flux"][0], 3 * 5  # per stage: the x-face and the y-face launch
     total = sum(v[0] for v in prof.values())
     s.close()
     return {"workload": WORKLOADS[wl]["name"], "fluid_cells": cells, "steps": steps, "ms_per_step": ms / steps,
@@ -530,7 +530,7 @@ def run_batch(args, rh, flops, torch, dist, world, rank, local):
     clocks = sampler.summary()
     k_prof = min(args.steps, 10)
     prof = b.profile_steps(k_prof, CFL)
-    flux_ms, flux_n = prof["flux"]
+    flux_ms, flux_n = prof["flux"][0], 3 * k_prof  # per stage: the x-face and the y-face launch
     achieved = fl_launch / (flux_ms / flux_n * 1e-3) / 1e12
     peak = rh.api.fp64_peak_tflops(local)
     total_prof_ms = sum(v[0] for v in prof.values())
@@ -541,7 +541,8 @@ def run_batch(args, rh, flops, torch, dist, world, rank, local):
     hbm, hbm_src = hbm_peak()
     g_achieved = g_bytes / (ghost_stage_ms * 1e-3) / 1e9
     bkey = "exact" if args.exact else "fma"
-    rl_flux = {"bound": "fp64", "kernel": "k_flux (x+y interface WENO5 fluxes, all instances)",
+    rl_flux = {"bound": "fp64", "kernel": "k_flux<0> + k_flux<1> (x and y interface WENO5 fluxes of one stage, "
+               "all instances)",
                "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                "traffic": None if FLUX_TRAFFIC_PER_FACE[bkey] is None else FLUX_TRAFFIC_PER_FACE[bkey] * n_faces,
                "traffic_unit": "bytes per launch", "peak_source": "measured DFMA loop on this GPU (rh3t_fp64_peak)",
@@ -722,7 +723,7 @@ def main():
 
     # roofline of the dominant kernel: live per-launch durations (CUDA events)
     prof = s.profile_steps(min(args.steps, 20), CFL)
-    flux_ms, flux_n = prof["flux"]
+    flux_ms, flux_n = prof["flux"][0], 3 * min(args.steps, 20)  # per stage: the x-face and the y-face launch
     fl_launch = flops.flux_launch_flops(nxf, nyf, diff)
     achieved = fl_launch / (flux_ms / flux_n * 1e-3) / 1e12
     peak = rh.api.fp64_peak_tflops(local)
@@ -763,7 +764,8 @@ def main():
                        "ghost_build_s": round(build_s, 3)},
             "arithmetic": "no FMA contraction, IEEE quotients, correctly rounded pow (the reference's "
                           "roundings)" if args.exact else "FMA contraction, shared reciprocals",
-            "roofline": {"bound": "fp64", "kernel": "k_flux (x+y interface WENO5 fluxes)", "achieved": achieved,
+            "roofline": {"bound": "fp64", "kernel": "k_flux<0> + k_flux<1> (x and y interface WENO5 fluxes of one "
+                         "stage)", "achieved": achieved,
                          "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                          "traffic": FLUX_TRAFFIC_BYTES["exact" if args.exact else "fma"].get(args.workload),
                          "traffic_unit": "bytes per launch",
