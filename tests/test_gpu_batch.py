@@ -31,7 +31,7 @@ def _mixed_fields(rh):
     ]
 
 
-def _alone(rh, f, g, nsteps, exact=False):
+def _alone(rh, f, g, nsteps, exact=True):
     s = rh.Solver(f, g, exact=exact)
     s.advance(nsteps, 0.05)
     u, t = s.download()
