@@ -633,6 +633,11 @@ def run_batch(args, rh, flops, torch, dist, world, rank, local):
                 "batched_speedup": value / plain_value},
             "adjoint": adj,
             "roofline": roofline,
+            "launch_gaps": {"graph_ms_per_step": ms / args.steps, "kernel_ms_per_step": total_prof_ms / k_prof,
+                            "gap_fraction": 1.0 - (total_prof_ms / k_prof) / (ms / args.steps),
+                            "note": "one step of the whole batch replays as one CUDA graph of "
+                                    f"{launches // args.steps} kernels; kernel_ms_per_step sums CUDA-event "
+                                    "durations of each kernel in eager profiled steps"},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": launches,
