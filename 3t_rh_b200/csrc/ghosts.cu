@@ -88,8 +88,12 @@ __device__ __forceinline__ void mbar_fence_init() {
 }
 
 // one thread: expect `bytes` on bar, then copy global -> shared (16-byte
-// aligned addresses, bytes a multiple of 16)
+// aligned addresses, bytes a multiple of 16). The buffer is reused: the
+// proxy fence orders the warp's earlier reads of it (generic proxy, made
+// visible to this thread by the __syncwarp before every call) before the
+// copy's writes (async proxy).
 __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, unsigned long long* bar) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
                  : "memory");
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
@@ -368,7 +372,7 @@ __device__ __forceinline__ void dot_pair(GhostWarp& G, const double* __restrict_
 __device__ __forceinline__ void heavy_ghost(const Inst* __restrict__ insts, const Inst& I, const GhostRec& Rg,
                                             GhostWarp& G, const double* __restrict__ rec,
                                             const double* __restrict__ hrec, int lane, int stage,
-                                            unsigned slot_a, unsigned slot_b, const double s0[6],
+                                            unsigned slot_a, unsigned slot_b, double dr, const double s0[6],
                                             const double s1[6], int n_heavy, int n_inst, double n0[6],
                                             double n1[6], bool& n_skip) {
     const DevParams& P = I.P;
@@ -398,8 +402,6 @@ __device__ __forceinline__ void heavy_ghost(const Inst* __restrict__ insts, cons
         nplane = insts[n_inst].plane;
         nerr = insts[n_inst].err;
     }
-    double dr = 0.0;
-    if (lane < 30) dr = rec[GH_D + lane - 5 * (lane / 5)];
     __syncwarp();
     // the record is not read below: bring in the next ghost's
     if (lane == 0 && n_heavy >= 0) bulk_load(G.rec[0], hrec + (size_t)n_heavy * GH_REC, GH_REC * 8, &G.bar[0]);
@@ -540,9 +542,12 @@ __global__ void __launch_bounds__(GH_WARPS * 32, GH_BLOCKS_PER_SM) k_ghosts(cons
                 return;
             }
             for (int e = lane; e < GH_LR; e += 32) G.LR[e] = G.rec[0][GH_L + e];
+            // d_r of lane (c, r), read here with L/R: every read of the record
+            // is then long complete when the next ghost's copy overwrites it
+            const double dr = lane < 30 ? G.rec[0][GH_D + lane - 5 * (lane / 5)] : 0.0;
             __syncwarp();
             if (!skip) {
-                heavy_ghost(insts, I, Rg, G, G.rec[0], hrec, lane, stage, slot_a, slot_b, s0, s1, n_heavy,
+                heavy_ghost(insts, I, Rg, G, G.rec[0], hrec, lane, stage, slot_a, slot_b, dr, s0, s1, n_heavy,
                             n_inst, n0, n1, n_skip);
             } else if (n_heavy >= 0) {
                 if (lane == 0) bulk_load(G.rec[0], hrec + (size_t)n_heavy * GH_REC, GH_REC * 8, &G.bar[0]);
