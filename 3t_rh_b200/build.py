@@ -25,7 +25,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CU_SOURCES = ["kernels.cu", "ghosts.cu", "flux.cu", "rhs.cu", "context.cu", "tune.cu", "adjoint.cu", "adjoint_host.cu", "noalloc.cu", "lsbuild.cu", "io.cu", "divcheck.cu"]
 CPP_SOURCES = ["host/ghostgrid.cpp"]
-HEADERS = ["physics.cuh", "rh3t_dev.h", "kernels.cuh", "common.cuh", "context.h", "dual.cuh", "ghost_rows.cuh", "divrn.cuh", "host/lsbuild.h"]
+HEADERS = ["physics.cuh", "rh3t_dev.h", "kernels.cuh", "common.cuh", "context.h", "dual.cuh", "ghost_rows.cuh", "divrn.cuh", "mbar.cuh", "host/lsbuild.h"]
 
 
 def _run(cmd):

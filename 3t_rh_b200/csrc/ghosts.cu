@@ -43,6 +43,7 @@
 #include "kernels.cuh"
 #include "physics.cuh"
 #include "ghost_rows.cuh"
+#include "mbar.cuh"
 
 namespace rh3t {
 
@@ -55,8 +56,6 @@ constexpr bool kExactG = false;
 constexpr int GH_WARPS = 4;
 constexpr int GH_BLOCKS_PER_SM = 3;
 constexpr int GH_PREP_THREADS = 64; // 41.6 KB of staging per block: 5 blocks per SM
-constexpr int GH_WAIT_LIMIT = 1 << 18; // try_wait rounds (about a second) before a wait counts as timed out
-constexpr int GH_TIMEOUT_CODE = 11;    // RH3T_ERR_DEVICE_TIMEOUT
 __constant__ int kStOff[6] = {0, 1, 5, 14, 30, 55};
 __constant__ int kSOff[6] = {0, 1, 17, 98, 354, 979};
 __constant__ int kWOff[6] = {0, 1, 9, 36, 100, 225};
@@ -76,17 +75,6 @@ constexpr int GH_SMEM = GH_WARPS * (int)sizeof(GhostWarp);
 constexpr int GH_LR_R = GH_R - GH_L, GH_LR_LAM = GH_LAM - GH_L;
 
 // ---------------------------------------------------------------- bulk copy
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(unsigned long long* bar) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
-}
-
-__device__ __forceinline__ void mbar_fence_init() {
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-
 // one thread: expect `bytes` on bar, then copy global -> shared (16-byte
 // aligned addresses, bytes a multiple of 16). The buffer is reused: the
 // proxy fence orders the warp's earlier reads of it (generic proxy, made
@@ -100,23 +88,6 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t b
                      smem_u32(dst)),
                  "l"(src), "r"(bytes), "r"(smem_u32(bar))
                  : "memory");
-}
-
-// bounded wait for the phase with parity `parity` of bar
-__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, uint32_t parity) {
-    const uint32_t a = smem_u32(bar);
-    for (int it = 0; it < GH_WAIT_LIMIT; ++it) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}"
-            : "=r"(done)
-            : "r"(a), "r"(parity)
-            : "memory");
-        if (done) return true;
-    }
-    return false;
 }
 
 // bc1.rs:467-469 solve6 with LAPACK getrf/getrs semantics
@@ -511,7 +482,7 @@ __global__ void __launch_bounds__(GH_WARPS * 32, GH_BLOCKS_PER_SM) k_ghosts(cons
     if (g < nh) { // warp-uniform
         const unsigned slot_a = kSlotA[lane], slot_b = kSlotB[lane];
         if (lane == 0) {
-            mbar_init(&G.bar[0]);
+            mbar_init(&G.bar[0], 1);
             mbar_fence_init();
             bulk_load(G.rec[0], hrec + (size_t)heavy[g].heavy * GH_REC, GH_REC * 8, &G.bar[0]);
         }
@@ -538,7 +509,7 @@ __global__ void __launch_bounds__(GH_WARPS * 32, GH_BLOCKS_PER_SM) k_ghosts(cons
             double n0[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, n1[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
             const bool ok = __all_sync(0xffffffffu, mbar_wait(&G.bar[0], (uint32_t)(it & 1)));
             if (!ok) {
-                if (lane == 0) report(I, 1 + 2 * stage, GH_TIMEOUT_CODE, (unsigned)Rg.gid);
+                if (lane == 0) report(I, 1 + 2 * stage, MBAR_TIMEOUT_CODE, (unsigned)Rg.gid);
                 return;
             }
             for (int e = lane; e < GH_LR; e += 32) G.LR[e] = G.rec[0][GH_L + e];
@@ -594,10 +565,10 @@ __global__ void k_wait_check(int arrive, int* out) {
     __shared__ unsigned long long bar;
     const int lane = threadIdx.x & 31;
     if (lane == 0) {
-        mbar_init(&bar);
+        mbar_init(&bar, 1);
         mbar_fence_init();
         if (arrive)
-            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&bar)) : "memory");
+            mbar_arrive(&bar);
     }
     __syncwarp();
     const bool ok = __all_sync(0xffffffffu, mbar_wait(&bar, 0u));
