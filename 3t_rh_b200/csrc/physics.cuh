@@ -102,7 +102,23 @@ __device__ __forceinline__ Prim prim_from_state(const double s[6], const DevPara
     return d;
 }
 
-// state.rs:245-276 te, ti, tr (diffusion and source only)
+// state.rs:245-276 te, ti, tr (diffusion and source only). r6e, r6i, ra:
+// the instance's divisors 6 cve, 6 cvi and a_rad with their reciprocals
+// (every quotient stays the IEEE one, divrn.cuh)
+__device__ __forceinline__ void temps_from_state(const double s[6], const DevParams& P, const Recip& r6e,
+                                                 const Recip& r6i, const Recip& ra, double& te, double& ti,
+                                                 double& tr) {
+    const Recip r0 = recip(s[0]);
+    double u = div_rn(s[1], r0), v = div_rn(s[2], r0);
+    double w2 = sqd(u) + sqd(v);
+    te = s[3] / (s[0] * P.cve) - div_rn(w2, r6e);
+    ti = s[4] / (s[0] * P.cvi) - div_rn(w2, r6i);
+    double er_term = div_rn(s[5], r0) - div6_rn(w2);
+    tr = cr_pow_quarter(div_rn(er_term * s[0], ra));
+}
+
+// the same values with plain IEEE divisions (callers without the instance's
+// reciprocals at hand)
 __device__ __forceinline__ void temps_from_state(const double s[6], const DevParams& P, double& te, double& ti,
                                                  double& tr) {
     const Recip r0 = recip(s[0]);

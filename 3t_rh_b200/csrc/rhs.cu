@@ -25,9 +25,28 @@ constexpr bool kExactR = true;
 constexpr bool kExactR = false;
 #endif
 
+// divisors shared by every cell of an instance: 60 dx, dx, 60 dy, dy
+// (noncon.rs:26-44, 315-331), 6 cve, 6 cvi, a_rad (state.rs:245-276)
+constexpr int RHS_NR = 7;
+__device__ __forceinline__ double rhs_divisor(const Inst& I, int k) {
+    switch (k) {
+    case 0: return 60.0 * I.dx;
+    case 1: return I.dx;
+    case 2: return 60.0 * I.dy;
+    case 3: return I.dy;
+    case 4: return 6.0 * I.P.cve;
+    case 5: return 6.0 * I.P.cvi;
+    default: return I.P.a_rad;
+    }
+}
+__device__ __forceinline__ Recip rhs_recip(const Inst& I, const double* sR, int k) {
+    return recip_of(rhs_divisor(I, k), sR[k]);
+}
+
 __global__ void __launch_bounds__(RHS_THREADS, 2) k_rhs_stage(const Inst* __restrict__ insts, const Tile* __restrict__ tiles,
                                                    int nt, int stage, int mode, double* __restrict__ rhs_out) {
     __shared__ double sP[5][RHS_NPT]; // pe, pi, pr, u, v
+    __shared__ double sR[RHS_NR];      // reciprocals of the instance's divisors (rhs_divisor)
     if (blockIdx.x >= nt) return;
     const Tile t = tiles[blockIdx.x];
     const Inst& I = insts[t.inst];
@@ -38,6 +57,7 @@ __global__ void __launch_bounds__(RHS_THREADS, 2) k_rhs_stage(const Inst* __rest
     const int nx = I.nx, ny = I.ny;
     const int TJ = 1 << t.lg, TI = RHS_THREADS >> t.lg;
     const int HJ = TJ + 8, NPT = (TI + 8) * HJ;
+    if (threadIdx.x < RHS_NR) sR[threadIdx.x] = __ddiv_rn(1.0, rhs_divisor(I, threadIdx.x));
     // ---- stage node primitives (tile + 4-node cross halo)
     for (int p = threadIdx.x; p < NPT; p += blockDim.x) {
         const int hi = p / HJ, hj = p - hi * HJ;
@@ -73,14 +93,14 @@ __global__ void __launch_bounds__(RHS_THREADS, 2) k_rhs_stage(const Inst* __rest
         const int p = hc + (q - 4) * HJ;
         pe[q] = sP[0][p]; pi[q] = sP[1][p]; pr[q] = sP[2][p]; vel[q] = sP[3][p];
     }
-    if (kExactR) noncon9(pe, pi, pr, vel, recip(60.0 * dx), recip(dx), ncx);
+    if (kExactR) noncon9(pe, pi, pr, vel, rhs_recip(I, sR, 0), rhs_recip(I, sR, 1), ncx);
     else fastm::noncon9(pe, pi, pr, vel, 1.0 / (60.0 * dx), 1.0 / dx, ncx);
 #pragma unroll
     for (int q = 0; q < 9; ++q) {
         const int p = hc + (q - 4);
         pe[q] = sP[0][p]; pi[q] = sP[1][p]; pr[q] = sP[2][p]; vel[q] = sP[4][p];
     }
-    if (kExactR) noncon9(pe, pi, pr, vel, recip(60.0 * dy), recip(dy), ncy);
+    if (kExactR) noncon9(pe, pi, pr, vel, rhs_recip(I, sR, 2), rhs_recip(I, sR, 3), ncy);
     else fastm::noncon9(pe, pi, pr, vel, 1.0 / (60.0 * dy), 1.0 / dy, ncy);
 #pragma unroll
     for (int k = 0; k < 3; ++k) rhs[3 + k] = rhs[3 + k] + ncx[k] + ncy[k];
@@ -88,7 +108,7 @@ __global__ void __launch_bounds__(RHS_THREADS, 2) k_rhs_stage(const Inst* __rest
         double s[6];
         load6(src, plane, n, s);
         double te, ti_, tr;
-        temps_from_state(s, P, te, ti_, tr);
+        temps_from_state(s, P, rhs_recip(I, sR, 4), rhs_recip(I, sR, 5), rhs_recip(I, sR, 6), te, ti_, tr);
         const double so[3] = {-P.omega_ei * (te - ti_) - P.omega_er * (pow4d(te) - pow4d(tr)),
                               P.omega_ei * (te - ti_), P.omega_er * (pow4d(te) - pow4d(tr))};
 #pragma unroll
@@ -139,10 +159,11 @@ __global__ void __launch_bounds__(RHS_THREADS, 2) k_rhs_stage(const Inst* __rest
     }
     bool ok = isfinite(v[0]) && isfinite(v[1]) && isfinite(v[2]) && isfinite(v[3]) && isfinite(v[4]) &&
               isfinite(v[5]) && v[0] > 0.0;
-    if (ok) {
-        const double ux = v[1] / v[0], uy = v[2] / v[0];
-        const double k = (ux * ux + uy * uy) / 6.0;
-        ok = !(v[3] / v[0] - k <= 0.0 || v[4] / v[0] - k <= 0.0 || v[5] / v[0] - k <= 0.0);
+    if (ok) { // main.rs:24-33, the five quotients by rho through one reciprocal (the same IEEE quotients)
+        const Recip r0 = recip(v[0]);
+        const double ux = div_rn(v[1], r0), uy = div_rn(v[2], r0);
+        const double k = div6_rn(ux * ux + uy * uy);
+        ok = !(div_rn(v[3], r0) - k <= 0.0 || div_rn(v[4], r0) - k <= 0.0 || div_rn(v[5], r0) - k <= 0.0);
     }
     if (!ok) report(I, 2 + 2 * stage, 1, (unsigned)((long long)i * ny + j));
 }

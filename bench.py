@@ -55,16 +55,22 @@ WORKLOADS = {
 }
 PLANAR_PARAMS = dict(kappa_e=1e-3, kappa_i=1e-3, kappa_r=1e-3, omega_ei=1.0, omega_er=1.0, periodic_ly=0.03125)
 CFL = 0.05
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_flux
-# launch, from an ncu capture of `bench.py --steps 3 --warmup 3 --no-cpu
-# --no-e2e` (FMA build); None where no capture exists
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one stage's
+# fluxes on a plain workload, from an ncu capture of `bench.py --steps 3
+# --warmup 3 --no-cpu --no-e2e` (FMA build, when x and y faces were one
+# launch); None where no capture exists
 FLUX_TRAFFIC_BYTES = {"fma": {"cyl961": 651.5e6}, "exact": {}}
 # DRAM bytes per heavy ghost of one stage's ghost update (k_ghost_prep +
-# k_ghosts) and per active face of one k_flux launch, from ncu captures on
-# the batch24 workload (84,000 heavy ghosts, 1,714,456 faces), scaled by the
-# heavy-ghost and face counts of the batched workloads
-GHOST_TRAFFIC_PER_HEAVY = {"fma": (902.88e6 + 7.24e6 + 15.32e6 + 9.25e6) / 84000, "exact": None}
-FLUX_TRAFFIC_PER_FACE = {"fma": (74.60e6 + 43.63e6) / 1714456, "exact": None}
+# k_ghosts) and per active face of one stage's k_flux<0> + k_flux<1>, from
+# ncu captures on the batch24 workload (84,000 heavy ghosts, 860,240 x and
+# 854,216 y faces), scaled by the heavy-ghost and face counts of the batched
+# workloads. The no-contraction capture holds k_ghosts and both flux
+# kernels; its ghost figure takes k_ghost_prep's bytes from the FMA-build
+# capture (the same loads and stores in both builds).
+GHOST_TRAFFIC_PER_HEAVY = {"fma": (902.88e6 + 7.24e6 + 15.32e6 + 9.25e6) / 84000,
+                           "exact": (903.11e6 + 7.75e6 + 15.32e6 + 9.25e6) / 84000}
+FLUX_TRAFFIC_PER_FACE = {"fma": (74.60e6 + 43.63e6) / 1714456,
+                         "exact": (48.58e6 + 12.24e6 + 45.42e6 + 7.69e6) / 1714456}
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -545,13 +551,21 @@ def run_batch(args, rh, flops, torch, dist, world, rank, local):
                "all instances)",
                "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                "traffic": None if FLUX_TRAFFIC_PER_FACE[bkey] is None else FLUX_TRAFFIC_PER_FACE[bkey] * n_faces,
-               "traffic_unit": "bytes per launch", "peak_source": "measured DFMA loop on this GPU (rh3t_fp64_peak)",
-               "flops_per_launch": fl_launch, "launch_ms": flux_ms / flux_n}
+               "traffic_unit": "bytes per stage (both launches)",
+               "peak_source": "measured DFMA loop on this GPU (rh3t_fp64_peak)",
+               "flops_per_stage": fl_launch, "stage_ms": flux_ms / flux_n, "launches_per_stage": 2,
+               "flop_count": "algorithmic: every add, sub, mul, div, sqrt of the reference's expressions = 1 "
+                             "(a division costs 3-14 FP64 issue slots here)"}
+    if args.exact:
+        # every product and sum of the reference issues on its own: an FP64
+        # stream without FMA peaks at half the DFMA FLOP rate
+        rl_flux["no_fma_ceiling"] = peak / 2.0
+        rl_flux["frac_of_no_fma_ceiling"] = achieved / (peak / 2.0)
     rl_ghost = {"bound": "hbm", "kernel": "k_ghost_prep + k_ghosts (one stage's ghost update, all instances)",
                 "achieved": g_achieved, "peak": hbm, "unit": "GB/s", "frac": g_achieved / hbm,
                 "traffic": None if GHOST_TRAFFIC_PER_HEAVY[bkey] is None else GHOST_TRAFFIC_PER_HEAVY[bkey] * n_heavy,
                 "traffic_unit": "bytes per stage", "peak_source": hbm_src,
-                "bytes_per_launch": g_bytes, "launch_ms": ghost_stage_ms,
+                "bytes_per_stage": g_bytes, "stage_ms": ghost_stage_ms,
                 "bytes_model": f"{flops.HEAVY_GHOST_BYTES} B of GhostBC tables per heavy ghost x {n_heavy}"}
     dominant = "ghosts" if share["ghosts"] >= share["flux"] else "flux"
     roofline = dict(rl_ghost if dominant == "ghosts" else rl_flux)
@@ -773,9 +787,11 @@ def main():
                          "stage)", "achieved": achieved,
                          "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                          "traffic": FLUX_TRAFFIC_BYTES["exact" if args.exact else "fma"].get(args.workload),
-                         "traffic_unit": "bytes per launch",
+                         "traffic_unit": "bytes per stage (both launches)",
                          "peak_source": "measured DFMA loop on this GPU (rh3t_fp64_peak)",
-                         "flops_per_launch": fl_launch, "launch_ms": flux_ms / flux_n,
+                         "flops_per_stage": fl_launch, "stage_ms": flux_ms / flux_n, "launches_per_stage": 2,
+                         **({"no_fma_ceiling": peak / 2.0, "frac_of_no_fma_ceiling": achieved / (peak / 2.0)}
+                            if args.exact else {}),
                          "kernel_share": {k: v[0] / total_prof_ms for k, v in prof.items()},
                          "step_tflops": step_fl / (ms / args.steps * 1e-3) / 1e12,
                          "step_flops": step_fl},
