@@ -27,8 +27,9 @@
 //
 // The argument needs no overflow, underflow or special value anywhere: the
 // fast sequence is taken only when both exponents are within [-250, 250]
-// (then z, y and r are normal numbers); anything else (zero, subnormal, huge,
-// infinite, NaN) takes the IEEE division. tests/test_gpu_math.py compares
+// (then z, y and r are normal numbers); a zero numerator over such a divisor
+// is the signed zero a y; anything else (subnormal, huge, infinite, NaN, a
+// divisor out of range) takes the IEEE division. tests/test_gpu_math.py compares
 // every routine here with the IEEE quotient bit for bit on random,
 // near-midpoint and special operands (rh3t_div_check).
 #pragma once
@@ -44,6 +45,17 @@ __device__ __forceinline__ bool div_in_range(double x) {
 // take it, and one copy of its code serves every call site (the callers'
 // code stays small enough for the instruction cache)
 static __device__ __noinline__ double div_ieee(double a, double b) { return __ddiv_rn(a, b); }
+
+// operands outside the fast range (b_ok: b is in it, y = RN(1/b)): a zero
+// numerator over such a divisor, common where a flow is uniform, gives the
+// signed zero a y (y is finite, nonzero and of b's sign, so the sign is a's
+// XOR b's, as in IEEE division); anything else takes the IEEE quotient. The
+// zero test is inline: zero numerators are too frequent for a call (batch
+// of half-cylinder instances: with zeros through the IEEE division the flux
+// kernels ran 9% and the RHS 26% slower, with the test out of line 2% and 6%)
+__device__ __forceinline__ double div_edge(double a, double b, double y, bool b_ok) {
+    return (b_ok && a == 0.0) ? __dmul_rn(a, y) : div_ieee(a, b);
+}
 
 struct Recip {
     double b, y;
@@ -69,7 +81,7 @@ __device__ __forceinline__ Recip recip_of(double b, double y) {
 
 // a / d.b, correctly rounded
 __device__ __forceinline__ double div_rn(double a, const Recip& d) {
-    if (!(d.ok && div_in_range(a))) return div_ieee(a, d.b);
+    if (!(d.ok && div_in_range(a))) return div_edge(a, d.b, d.y, d.ok);
     double q = __dmul_rn(a, d.y);
     double r = __fma_rn(-d.b, q, a);
     q = __fma_rn(r, d.y, q);
@@ -79,15 +91,15 @@ __device__ __forceinline__ double div_rn(double a, const Recip& d) {
 
 // a / 3.0 and a / 6.0, correctly rounded
 __device__ __forceinline__ double div3_rn(double a) {
-    if (!div_in_range(a)) return div_ieee(a, 3.0);
     const double y = 0x1.5555555555555p-2; // RN(1/3)
+    if (!div_in_range(a)) return div_edge(a, 3.0, y, true);
     const double q = __dmul_rn(a, y);
     const double r = __fma_rn(-3.0, q, a);
     return __fma_rn(r, y, q);
 }
 __device__ __forceinline__ double div6_rn(double a) {
-    if (!div_in_range(a)) return div_ieee(a, 6.0);
     const double y = 0x1.5555555555555p-3; // RN(1/6)
+    if (!div_in_range(a)) return div_edge(a, 6.0, y, true);
     const double q = __dmul_rn(a, y);
     const double r = __fma_rn(-6.0, q, a);
     return __fma_rn(r, y, q);
