@@ -51,8 +51,8 @@ __global__ void k_div_check(long long n, unsigned long long seed, unsigned long 
         const uint64_t h1 = mix64(seed ^ (uint64_t)k), h2 = mix64(h1), h3 = mix64(h2);
         double a, b, got;
         if (cat == 0) {
-            a = make_double(h1, (int)(h3 % 541) - 270);
-            b = make_double(h2, (int)((h3 >> 16) % 541) - 270);
+            a = make_double(h1, (int)(h3 % 941) - 470);
+            b = make_double(h2, (int)((h3 >> 16) % 941) - 470);
         } else if (cat == 1) {
             a = make_double(h1, (int)(h3 % 401) - 200);
             const uint64_t frac = 0x000fffffffffffffull - (h2 & 0xffull) - (((h3 >> 40) & 1) ? ((h2 >> 8) & 0xffffull) : 0);
@@ -62,15 +62,16 @@ __global__ void k_div_check(long long n, unsigned long long seed, unsigned long 
             a = near_midpoint(b, h2, (int)((h3 >> 16) % 201) - 100, (int)((h3 >> 40) % 7) - 3);
         } else if (cat == 3) {
             const double specials[12] = {0.0, -0.0, INFINITY, -INFINITY, NAN, 4.9e-324, 2.2250738585072014e-308,
-                                         1.7976931348623157e308, 0x1p-250, 0x1p250, 0x1.fffffffffffffp-251,
-                                         0x1p251};
+                                         1.7976931348623157e308, 0x1p-450, 0x1p450, 0x1.fffffffffffffp-451,
+                                         0x1.fffffffffffffp450};
             a = (h3 & 3) == 0 ? specials[h1 % 12] : make_double(h1, (int)(h3 % 2047) - 1023);
             b = (h3 & 12) == 0 ? specials[h2 % 12] : make_double(h2, (int)((h3 >> 16) % 2047) - 1023);
-            if ((h3 >> 20) % 5 == 0) a = make_double(h1, (int)((h3 >> 24) % 7) + 247);
-            if ((h3 >> 28) % 5 == 0) b = make_double(h2, -(int)((h3 >> 32) % 7) - 247);
+            // next to the fast path's exponent range [-450, 450], on both sides
+            if ((h3 >> 20) % 5 == 0) a = make_double(h1, ((h3 >> 44) & 1 ? 1 : -1) * ((int)((h3 >> 24) % 7) + 447));
+            if ((h3 >> 28) % 5 == 0) b = make_double(h2, ((h3 >> 45) & 1 ? 1 : -1) * ((int)((h3 >> 32) % 7) + 447));
         } else {
             b = cat == 4 ? 3.0 : 6.0;
-            if ((h3 & 1) == 0) a = make_double(h1, (int)(h3 % 601) - 300);
+            if ((h3 & 1) == 0) a = make_double(h1, (int)(h3 % 1001) - 500);
             else a = near_midpoint(b, h2, (int)((h3 >> 16) % 201) - 100, (int)((h3 >> 40) % 7) - 3);
         }
         const double want = __ddiv_rn(a, b);

@@ -26,8 +26,9 @@
 // faithful: one correction suffices.
 //
 // The argument needs no overflow, underflow or special value anywhere: the
-// fast sequence is taken only when both exponents are within [-250, 250]
-// (then z, y and r are normal numbers); a zero numerator over such a divisor
+// fast sequence is taken only when both exponents are within [-450, 450]
+// (then z lies in [2^-901, 2^901], y in [2^-451, 2^450] and a nonzero r
+// above 2^-557: all normal numbers); a zero numerator over such a divisor
 // is the signed zero a y; anything else (subnormal, huge, infinite, NaN, a
 // divisor out of range) takes the IEEE division. tests/test_gpu_math.py compares
 // every routine here with the IEEE quotient bit for bit on random,
@@ -38,7 +39,7 @@ namespace rh3t {
 
 __device__ __forceinline__ bool div_in_range(double x) {
     const unsigned e = (unsigned)__double2hiint(x) & 0x7ff00000u;
-    return e - 0x30500000u <= 0x1f400000u; // biased exponent in [1023 - 250, 1023 + 250]
+    return e - 0x23d00000u <= 0x38400000u; // biased exponent in [1023 - 450, 1023 + 450]
 }
 
 // the IEEE quotient, out of line: the rare operands outside the fast range
