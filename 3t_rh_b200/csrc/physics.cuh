@@ -299,35 +299,41 @@ __device__ __forceinline__ void r_row(int row, const Roe& q, const DevParams& P,
     const double u = q.u, v = q.v, w2 = q.w2, cs = q.cs;
     const double vel = DIR == 0 ? u : v;
     lam = row == 0 ? vel - cs : (row == 5 ? vel + cs : vel);
-    if (DIR == 0) {
+    if (row >= 3) {
+        // energy components k = 0, 1, 2 (e, i, r): one code path with the
+        // component's operands. Entries 0 and 5: Gk ek + w2/6 -+ vel cs / 3;
+        // the three others (x faces 1..3, y faces 2..4) hold gt w2 / (6 gk)
+        // at position k and +-gl (l the third index, + for position
+        // (k + 2) mod 3) elsewhere; the remaining entry is v / 3 (x faces,
+        // position 4) or u / 3 (y faces, position 1)
+        const int k = row - 3;
+        const double Gk = k == 0 ? GE : (k == 1 ? GI : GR);
+        const double ek = k == 0 ? q.ee : (k == 1 ? q.ei : q.er);
+        const double gk = k == 0 ? ge : (k == 1 ? gi : gr);
+        const double base = Gk * ek + div6_rn(w2);
+        const double vc = div3_rn(vel * cs);
+        R[0] = base - vc;
+        R[5] = base + vc;
+        const double dk = gt * w2 / (6.0 * gk);
+        const int o = DIR == 0 ? 1 : 2;
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+            const int l = 3 - k - m;
+            const double gl = l == 0 ? ge : (l == 1 ? gi : gr);
+            R[o + m] = m == k ? dk : (m == (k + 2) % 3 ? gl : -gl);
+        }
+        R[DIR == 0 ? 4 : 1] = div3_rn(DIR == 0 ? v : u);
+    } else if (DIR == 0) {
         switch (row) {
         case 0: R[0] = 1.0; R[1] = 1.0; R[2] = 1.0; R[3] = 1.0; R[4] = 0.0; R[5] = 1.0; break;
         case 1: R[0] = u - cs; R[1] = u; R[2] = u; R[3] = u; R[4] = 0.0; R[5] = u + cs; break;
-        case 2: R[0] = v; R[1] = v; R[2] = v; R[3] = v; R[4] = 1.0; R[5] = v; break;
-        case 3:
-            R[0] = GE * q.ee + div6_rn(w2) - div3_rn(u * cs); R[1] = gt * w2 / (6.0 * ge); R[2] = -gr; R[3] = gi;
-            R[4] = div3_rn(v); R[5] = GE * q.ee + div6_rn(w2) + div3_rn(u * cs); break;
-        case 4:
-            R[0] = GI * q.ei + div6_rn(w2) - div3_rn(u * cs); R[1] = gr; R[2] = gt * w2 / (6.0 * gi); R[3] = -ge;
-            R[4] = div3_rn(v); R[5] = GI * q.ei + div6_rn(w2) + div3_rn(u * cs); break;
-        default:
-            R[0] = GR * q.er + div6_rn(w2) - div3_rn(u * cs); R[1] = -gi; R[2] = ge; R[3] = gt * w2 / (6.0 * gr);
-            R[4] = div3_rn(v); R[5] = GR * q.er + div6_rn(w2) + div3_rn(u * cs); break;
+        default: R[0] = v; R[1] = v; R[2] = v; R[3] = v; R[4] = 1.0; R[5] = v; break;
         }
     } else {
         switch (row) {
         case 0: R[0] = 1.0; R[1] = 0.0; R[2] = 1.0; R[3] = 1.0; R[4] = 1.0; R[5] = 1.0; break;
         case 1: R[0] = u; R[1] = 1.0; R[2] = u; R[3] = u; R[4] = u; R[5] = u; break;
-        case 2: R[0] = v - cs; R[1] = 0.0; R[2] = v; R[3] = v; R[4] = v; R[5] = v + cs; break;
-        case 3:
-            R[0] = GE * q.ee + div6_rn(w2) - div3_rn(v * cs); R[1] = div3_rn(u); R[2] = gt * w2 / (6.0 * ge); R[3] = -gr;
-            R[4] = gi; R[5] = GE * q.ee + div6_rn(w2) + div3_rn(v * cs); break;
-        case 4:
-            R[0] = GI * q.ei + div6_rn(w2) - div3_rn(v * cs); R[1] = div3_rn(u); R[2] = gr; R[3] = gt * w2 / (6.0 * gi);
-            R[4] = -ge; R[5] = GI * q.ei + div6_rn(w2) + div3_rn(v * cs); break;
-        default:
-            R[0] = GR * q.er + div6_rn(w2) - div3_rn(v * cs); R[1] = div3_rn(u); R[2] = -gi; R[3] = ge;
-            R[4] = gt * w2 / (6.0 * gr); R[5] = GR * q.er + div6_rn(w2) + div3_rn(v * cs); break;
+        default: R[0] = v - cs; R[1] = 0.0; R[2] = v; R[3] = v; R[4] = v; R[5] = v + cs; break;
         }
     }
 }
@@ -367,14 +373,17 @@ __device__ __forceinline__ void l_row(int row, const Roe& q, const RoeDiv& rd, c
         mode = row;
     }
     if (mode == 0 || mode == 5) {
+        // the two acoustic rows differ only in the sign of one term of two
+        // entries: x + s y with s = +-1 is x + y or x - y exactly
+        const double s = mode == 0 ? 1.0 : -1.0;
         if (DIR == 0) {
-            L[0] = mode == 0 ? div_rn(gt * w2 + 6.0 * u * cs, rd.den) : div_rn(gt * w2 - 6.0 * u * cs, rd.den);
-            L[1] = mode == 0 ? div_rn(-2.0 * gt * u - 6.0 * cs, rd.den) : div_rn(-2.0 * gt * u + 6.0 * cs, rd.den);
+            L[0] = div_rn(gt * w2 + s * (6.0 * u * cs), rd.den);
+            L[1] = div_rn(-2.0 * gt * u + -s * (6.0 * cs), rd.den);
             L[2] = div_rn(-2.0 * gt * v, rd.den);
         } else {
-            L[0] = mode == 0 ? div_rn(gt * w2 + 6.0 * v * cs, rd.den) : div_rn(gt * w2 - 6.0 * v * cs, rd.den);
+            L[0] = div_rn(gt * w2 + s * (6.0 * v * cs), rd.den);
             L[1] = div_rn(-2.0 * gt * u, rd.den);
-            L[2] = mode == 0 ? div_rn(-2.0 * gt * v - 6.0 * cs, rd.den) : div_rn(-2.0 * gt * v + 6.0 * cs, rd.den);
+            L[2] = div_rn(-2.0 * gt * v + -s * (6.0 * cs), rd.den);
         }
         L[3] = div_rn(6.0 * ge, rd.den);
         L[4] = div_rn(6.0 * gi, rd.den);
@@ -384,23 +393,28 @@ __device__ __forceinline__ void l_row(int row, const Roe& q, const RoeDiv& rd, c
         else { L[0] = -u; L[1] = 1.0; L[2] = 0.0; }
         L[3] = 0.0; L[4] = 0.0; L[5] = 0.0;
     } else {
-        const double gk = mode == 2 ? ge : (mode == 3 ? gi : gr);
-        const double hk = mode == 2 ? q.he : (mode == 3 ? q.hi : q.hr);
+        // energy rows: k = 0, 1, 2 for e, i, r (modes 2, 3, 4), one code path
+        // with the mode's operands. Entry 3 + j: on the diagonal (j == k)
+        // -gk^2 / (gt cs2) - 6 gk / b (gk hk - gt cs2 w2); off it, with l the
+        // third index, -gk gj / (gt cs2) - 6 gk gj / b (hk +- 6 gl cs2), the
+        // sign + for j == (k + 2) mod 3: the reference's rows written per
+        // mode, the same products in the same order
+        const int k = mode - 2;
+        const double gk = k == 0 ? ge : (k == 1 ? gi : gr);
+        const double hk = k == 0 ? q.he : (k == 1 ? q.hi : q.hr);
         L[0] = div_rn(gk, rd.gt) - div_rn(gk * w2, rd.c6) - div_rn(gk * gt * w2, rd.b) * (hk - cs2 * w2);
         L[1] = div_rn(gk * u, rd.c3) + div_rn(2.0 * gk * gt * u, rd.b) * (hk - cs2 * w2);
         L[2] = div_rn(gk * v, rd.c3) + div_rn(2.0 * gk * gt * v, rd.b) * (hk - cs2 * w2);
-        if (mode == 2) {
-            L[3] = div_rn(-sqd(ge), rd.cg) - div_rn(6.0 * ge, rd.b) * (ge * hk - gt * cs2 * w2);
-            L[4] = div_rn(-ge * gi, rd.cg) - div_rn(6.0 * ge * gi, rd.b) * (hk - 6.0 * gr * cs2);
-            L[5] = div_rn(-ge * gr, rd.cg) - div_rn(6.0 * ge * gr, rd.b) * (hk + 6.0 * gi * cs2);
-        } else if (mode == 3) {
-            L[3] = div_rn(-gi * ge, rd.cg) - div_rn(6.0 * gi * ge, rd.b) * (hk + 6.0 * gr * cs2);
-            L[4] = div_rn(-sqd(gi), rd.cg) - div_rn(6.0 * gi, rd.b) * (gi * hk - gt * cs2 * w2);
-            L[5] = div_rn(-gi * gr, rd.cg) - div_rn(6.0 * gi * gr, rd.b) * (hk - 6.0 * ge * cs2);
-        } else {
-            L[3] = div_rn(-gr * ge, rd.cg) - div_rn(6.0 * gr * ge, rd.b) * (hk - 6.0 * gi * cs2);
-            L[4] = div_rn(-gr * gi, rd.cg) - div_rn(6.0 * gr * gi, rd.b) * (hk + 6.0 * ge * cs2);
-            L[5] = div_rn(-sqd(gr), rd.cg) - div_rn(6.0 * gr, rd.b) * (gr * hk - gt * cs2 * w2);
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const bool diag = j == k;
+            const int l = 3 - k - j;
+            const double gj = j == 0 ? ge : (j == 1 ? gi : gr);
+            const double gl = l == 0 ? ge : (l == 1 ? gi : gr);
+            const double t = 6.0 * gl * cs2;
+            const double n2 = diag ? 6.0 * gk : 6.0 * gk * gj;
+            const double f = diag ? gk * hk - gt * cs2 * w2 : hk + (j == (k + 2) % 3 ? t : -t);
+            L[3 + j] = div_rn(-gk * gj, rd.cg) - div_rn(n2, rd.b) * f;
         }
     }
 }
