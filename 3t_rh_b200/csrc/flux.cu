@@ -108,6 +108,30 @@ __device__ __forceinline__ double char_flux(const FluxShared& S, const DevParams
     return weno5_any(fp[0], fp[1], fp[2], fp[3], fp[4], P.eps) + weno5_any(fm[5], fm[4], fm[3], fm[2], fm[1], P.eps);
 }
 
+// The diffusion terms (off in most runs) are out of line: their code stays
+// out of the instruction cache of runs without diffusion.
+// diffusion.rs:27-50: component 3 <- Te, 4 <- Ti, 5 <- Tr^4 (m3 = 0, 1, 2)
+static __device__ __noinline__ void diffusion_out(const FluxShared& S, const DevParams& P, int m3, int p0, int ps,
+                                                  double* out) {
+    double v[6];
+#pragma unroll
+    for (int m = 0; m < 6; ++m) {
+        const double x = S.T[m3][p0 + m * ps];
+        v[m] = m3 == 2 ? pow4d(x) : x;
+    }
+    const double kap = m3 == 0 ? P.kappa_e : (m3 == 1 ? P.kappa_i : P.kappa_r);
+    const double term = kap * (2.0 * v[5] - 25.0 * v[4] + 245.0 * v[3] - 245.0 * v[2] + 25.0 * v[1] - 2.0 * v[0]);
+    *out = term / 180.0;
+}
+
+// temperatures of staged point p (its state was written to S.U by this thread)
+static __device__ __noinline__ void stage_temps(FluxShared& S, int p, const DevParams& P) {
+    const double s[6] = {S.U[0][p].x, S.U[0][p].y, S.U[1][p].x, S.U[1][p].y, S.U[2][p].x, S.U[2][p].y};
+    double te, ti, tr;
+    temps_from_state(s, P, te, ti, tr);
+    S.T[0][p] = te; S.T[1][p] = ti; S.T[2][p] = tr;
+}
+
 template <int DIR>
 __device__ __forceinline__ void face_out(const Inst& I, const FluxShared& S, const Tile& t, int k, int f) {
     const DevParams& P = I.P;
@@ -126,19 +150,7 @@ __device__ __forceinline__ void face_out(const Inst& I, const FluxShared& S, con
     if (DIR == 0) { fplane = (long long)(nx + 1) * ny; fidx = (long long)i * ny + j; fo = I.fx; dfo = I.dfx; }
     else { fplane = (long long)nx * (ny + 1); fidx = (long long)i * (ny + 1) + j; fo = I.fy; dfo = I.dfy; }
     fo[k * fplane + fidx] = out;
-    if (I.diffusion && k >= 3) {
-        // diffusion.rs:27-50: component 3 <- Te, 4 <- Ti, 5 <- Tr^4
-        const int m3 = k - 3;
-        double v[6];
-#pragma unroll
-        for (int m = 0; m < 6; ++m) {
-            const double x = S.T[m3][p0 + m * ps];
-            v[m] = m3 == 2 ? pow4d(x) : x;
-        }
-        const double kap = m3 == 0 ? P.kappa_e : (m3 == 1 ? P.kappa_i : P.kappa_r);
-        const double term = kap * (2.0 * v[5] - 25.0 * v[4] + 245.0 * v[3] - 245.0 * v[2] + 25.0 * v[1] - 2.0 * v[0]);
-        dfo[m3 * fplane + fidx] = term / 180.0;
-    }
+    if (I.diffusion && k >= 3) diffusion_out(S, P, k - 3, p0, ps, dfo + (k - 3) * fplane + fidx);
 }
 
 template <int DIR>
@@ -167,11 +179,7 @@ __device__ __forceinline__ void flux_tile(const Inst& I, const Tile& t, int stag
             S.F[k][p] = make_double2(f[2 * k], f[2 * k + 1]);
         }
         S.PR[0][p] = d.u; S.PR[1][p] = d.v; S.PR[2][p] = d.e_e; S.PR[3][p] = d.e_i; S.PR[4][p] = d.e_r;
-        if (diff) {
-            double te, ti, tr;
-            temps_from_state(s, P, te, ti, tr);
-            S.T[0][p] = te; S.T[1][p] = ti; S.T[2][p] = tr;
-        }
+        if (diff) stage_temps(S, p, P);
     }
     __syncthreads();
     for (int f = threadIdx.x; f < FLUX_FACES; f += blockDim.x) {
@@ -216,8 +224,10 @@ __device__ __forceinline__ void flux_tile(const Inst& I, const Tile& t, int stag
     const int c = threadIdx.x >> 5, lane = threadIdx.x & 31; // warp-uniform characteristic field
     Recip rgt = {1.0, 1.0, false};
     if (kExact) rgt = recip((P.gamma_i - 1.0) + (P.gamma_e - 1.0) + (P.gamma_r - 1.0));
-    // ---- 2. characteristic pass: field c of faces lane and lane + 32
-#pragma unroll
+    // ---- 2. characteristic pass: field c of faces lane and lane + 32 (a
+    // loop, not unrolled: one copy of the pass's code keeps the kernel
+    // within the instruction cache)
+#pragma unroll 1
     for (int h = 0; h < FLUX_FACES / 32; ++h) {
         const int f = lane + 32 * h;
         if (S.act[f]) {
@@ -228,7 +238,7 @@ __device__ __forceinline__ void flux_tile(const Inst& I, const Tile& t, int stag
     }
     __syncthreads();
     // ---- 3. output pass: component k = c
-#pragma unroll
+#pragma unroll 1
     for (int h = 0; h < FLUX_FACES / 32; ++h) {
         const int f = lane + 32 * h;
         if (S.act[f]) face_out<DIR>(I, S, t, c, f);
