@@ -177,6 +177,15 @@ __device__ __forceinline__ Roe roe_average(double rho_s1, const Prim& d3, double
     return q;
 }
 
+// Mode of left eigenvector row `row`: 0 acoustic-, 1 transverse, 2 electron,
+// 3 ion, 4 radiation, 5 acoustic+. x faces order their rows
+// [u-c, e, i, r, transverse, u+c], y faces [v-c, transverse, e, i, r, v+c].
+// (Selects, not a table: a table indexed by a runtime row lives in local memory.)
+template <int DIR> __device__ __forceinline__ int row_mode(int row) {
+    if (DIR != 0) return row;
+    return row == 0 ? 0 : (row == 5 ? 5 : (row == 4 ? 1 : row + 1));
+}
+
 // Row `row` of the left eigenvector matrix (weno.rs:79-458). DIR 0: rows
 // [u-c, e, i, r, transverse, u+c]; DIR 1: [v-c, transverse, e, i, r, v+c].
 // Written over the scalar type T (double; a dual-number type in the adjoint).
@@ -186,15 +195,7 @@ __device__ __forceinline__ void l_row(int row, const RoeT<T>& q, const DevParams
     const double gi = GI - 1.0, ge = GE - 1.0, gr = GR - 1.0;
     const double gt = gi + ge + gr;
     const T u = q.u, v = q.v, w2 = q.w2, cs = q.cs, cs2 = q.cs2, b = q.b, den = q.den;
-    // map to a mode: 0 acoustic-, 1 transverse, 2 electron, 3 ion, 4 radiation, 5 acoustic+
-    int mode;
-    if (DIR == 0) {
-        const int m[6] = {0, 2, 3, 4, 1, 5};
-        mode = m[row];
-    } else {
-        const int m[6] = {0, 1, 2, 3, 4, 5};
-        mode = m[row];
-    }
+    const int mode = row_mode<DIR>(row);
     if (mode == 0 || mode == 5) {
         const double sgn = mode == 0 ? 1.0 : -1.0;
         if (DIR == 0) {
@@ -365,13 +366,7 @@ __device__ __forceinline__ void l_row(int row, const Roe& q, const RoeDiv& rd, c
     const double gi = GI - 1.0, ge = GE - 1.0, gr = GR - 1.0;
     const double gt = gi + ge + gr;
     const double u = q.u, v = q.v, w2 = q.w2, cs = q.cs, cs2 = q.cs2;
-    int mode;
-    if (DIR == 0) {
-        const int m[6] = {0, 2, 3, 4, 1, 5};
-        mode = m[row];
-    } else {
-        mode = row;
-    }
+    const int mode = row_mode<DIR>(row);
     if (mode == 0 || mode == 5) {
         // the two acoustic rows differ only in the sign of one term of two
         // entries: x + s y with s = +-1 is x + y or x - y exactly
@@ -474,13 +469,7 @@ __device__ __forceinline__ void l_row(int row, const Roe& q, double ics2, double
     const double gt = gi + ge + gr;
     const double u = q.u, v = q.v, w2 = q.w2, cs = q.cs, cs2 = q.cs2;
     const double iden = ics2 * (1.0 / 12.0);
-    int mode;
-    if (DIR == 0) {
-        const int m[6] = {0, 2, 3, 4, 1, 5};
-        mode = m[row];
-    } else {
-        mode = row;
-    }
+    const int mode = row_mode<DIR>(row);
     if (mode == 0 || mode == 5) {
         const double sg = mode == 0 ? 6.0 : -6.0;
         const double vn = DIR == 0 ? u : v;
@@ -544,9 +533,8 @@ __device__ __forceinline__ double weno5(double u0, double u1, double u2, double 
 
 } // namespace fastm
 
-// weno.rs:847-886 weno5 (WENO-JS, p = 2); out of line: a face's twelve
-// reconstructions share one copy of its code
-static __device__ __noinline__ double weno5(double u0, double u1, double u2, double u3, double u4, double eps) {
+// weno.rs:847-886 weno5 (WENO-JS, p = 2)
+__device__ __forceinline__ double weno5(double u0, double u1, double u2, double u3, double u4, double eps) {
     double beta2 = 13.0 / 12.0 * sqd(u2 - 2.0 * u3 + u4) + 0.25 * sqd(3.0 * u2 - 4.0 * u3 + u4);
     double beta1 = 13.0 / 12.0 * sqd(u1 - 2.0 * u2 + u3) + 0.25 * sqd(u1 - u3);
     double beta0 = 13.0 / 12.0 * sqd(u0 - 2.0 * u1 + u2) + 0.25 * sqd(u0 - 4.0 * u1 + 3.0 * u2);
