@@ -2,12 +2,13 @@
 // divrn.cuh against the IEEE quotient, bit for bit, on operands generated on
 // the device: random ones, divisors with all-ones significands, quotients
 // next to a rounding midpoint, operands at and beyond the fast path's
-// exponent range, and special values.
+// exponent range, and special values; and the reciprocals of a face's
+// L-row divisors that roe_div (physics.cuh) forms by scaling 1/(12 c^2).
 #include <cstdint>
 
 #include <cuda_runtime.h>
 
-#include "divrn.cuh"
+#include "physics.cuh"
 
 namespace rh3t {
 
@@ -40,10 +41,12 @@ __device__ __forceinline__ bool same_bits(double x, double y) {
     return __double_as_longlong(x) == __double_as_longlong(y);
 }
 
-constexpr int DIV_CATEGORIES = 6;
+constexpr int DIV_CATEGORIES = 7;
 
 // category of case k: 0 random, 1 all-ones divisors, 2 near-midpoint
-// quotients, 3 range edges and special values, 4 a / 3, 5 a / 6
+// quotients, 3 range edges and special values, 4 a / 3, 5 a / 6, 6 the
+// reciprocals of 6 c^2 and 3 c^2 in roe_div (c^2 > 0 with exponents over and
+// beyond the fast range, all-ones significands among them)
 __global__ void k_div_check(long long n, unsigned long long seed, unsigned long long* bad, double* first) {
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += stride) {
@@ -69,6 +72,31 @@ __global__ void k_div_check(long long n, unsigned long long seed, unsigned long 
             // next to the fast path's exponent range [-450, 450], on both sides
             if ((h3 >> 20) % 5 == 0) a = make_double(h1, ((h3 >> 44) & 1 ? 1 : -1) * ((int)((h3 >> 24) % 7) + 447));
             if ((h3 >> 28) % 5 == 0) b = make_double(h2, ((h3 >> 45) & 1 ? 1 : -1) * ((int)((h3 >> 32) % 7) + 447));
+        } else if (cat == 6) {
+            uint64_t hc = h1 & ~(1ull << 63);
+            if ((h3 & 7) == 0) hc |= 0x000fffffffffffffull;
+            const double cs2 = make_double(hc, (int)(h3 % 921) - 460);
+            Roe q{};
+            q.cs2 = cs2;
+            q.den = 12.0 * cs2;
+            q.b = 1.0;
+            DevParams P{};
+            P.gamma_e = 5.0 / 3.0;
+            P.gamma_i = 5.0 / 3.0;
+            P.gamma_r = 4.0 / 3.0;
+            const RoeDiv rd = roe_div(q, P);
+            const double w6 = __ddiv_rn(1.0, 6.0 * cs2), w3 = __ddiv_rn(1.0, 3.0 * cs2);
+            a = cs2;
+            b = 6.0 * cs2;
+            if (!same_bits(rd.c6.y, w6) || !same_bits(rd.c3.y, w3) || rd.c6.b != 6.0 * cs2 || rd.c3.b != 3.0 * cs2) {
+                atomicAdd(&bad[cat], 1ull);
+                if (atomicAdd(&bad[DIV_CATEGORIES], 1ull) == 0) {
+                    first[0] = a;
+                    first[1] = b;
+                    first[2] = same_bits(rd.c6.y, w6) ? rd.c3.y : rd.c6.y;
+                }
+            }
+            continue;
         } else {
             b = cat == 4 ? 3.0 : 6.0;
             if ((h3 & 1) == 0) a = make_double(h1, (int)(h3 % 1001) - 500);
@@ -91,9 +119,11 @@ __global__ void k_div_check(long long n, unsigned long long seed, unsigned long 
 
 } // namespace rh3t
 
-// counts[0..5]: mismatches per category (0 random, 1 all-ones divisors, 2
+// counts[0..6]: mismatches per category (0 random, 1 all-ones divisors, 2
 // near-midpoint quotients, 3 range edges and special values, 4 a / 3,
-// 5 a / 6); first[3]: a, b and the routine's quotient of one mismatch
+// 5 a / 6, 6 roe_div's reciprocals of 6 c^2 and 3 c^2); first[3]: a, b and
+// the routine's quotient of one mismatch (category 6: c^2, 6 c^2 and the
+// reciprocal)
 extern "C" int rh3t_div_check(int32_t device, int64_t n, uint64_t seed, int64_t* counts, double* first) {
     if (!counts || !first || n < 0) return 7; // RH3T_ERR_INVALID_ARGUMENT
     int ndev = 0;

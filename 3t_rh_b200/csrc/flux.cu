@@ -8,13 +8,13 @@
 //      shared memory once (the reference evaluates them once per face, six
 //      times per point); then each face's Roe state, from the staged
 //      primitives of its points 3 and 2, and its activity flag;
-//   2. characteristic pass: warp c owns characteristic field c for the 64
-//      faces (two per lane), so the row of L, the projections and the two
-//      WENO5 reconstructions of f+ and f- are warp-uniform code; g_c goes to
-//      shared memory;
-//   3. output pass: warp k owns component k and returns
-//      (R g)_k = sum_c R[k][c] g_c in the reference's summation order
-//      (weno.rs:793, 834-843), plus the diffusion flux for k >= 3.
+//   2. characteristic pass: a warp takes one characteristic field c for
+//      32 faces (one per lane) at a time, two (field, half) pairs per warp,
+//      so the row of L, the projections and the two WENO5 reconstructions
+//      of f+ and f- are warp-uniform code; g_c goes to shared memory;
+//   3. output pass: likewise one component k for 32 faces at a time,
+//      returning (R g)_k = sum_c R[k][c] g_c in the reference's summation
+//      order (weno.rs:793, 834-843), plus the diffusion flux for k >= 3.
 // Point data sit in shared memory as component pairs (double2), so a lane
 // reads a point's state and flux with six 16-byte loads.
 //
@@ -235,7 +235,15 @@ __device__ __forceinline__ void flux_tile(const Inst& I, const Tile& t, int stag
         for (int k = 0; k < NQ; ++k) S.Q[k][f] = qv[k];
     }
     __syncthreads();
-    const int c = threadIdx.x >> 5, lane = threadIdx.x & 31; // warp-uniform characteristic field
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // Each warp takes one heavy and one light half in both passes, so the
+    // six warps reach the barrier (and the block's end) together: the energy
+    // fields' L rows hold most of a face's divisions (x faces: fields 1-3,
+    // 0 and 5 acoustic, 4 transverse; y faces: 2-4, 0 and 5, 1), and so do
+    // the energy components' R rows (3-5). Field of warp w for faces 0..31
+    // and 32..63, one hex digit per warp:
+    constexpr unsigned kC0 = DIR == 0 ? 0x450321u : 0x150432u;
+    constexpr unsigned kC1 = DIR == 0 ? 0x321450u : 0x432150u;
     Recip rgt = {1.0, 1.0, false};
     if (kExact) rgt = recip((P.gamma_i - 1.0) + (P.gamma_e - 1.0) + (P.gamma_r - 1.0));
     // ---- 2. characteristic pass: field c of faces lane and lane + 32 (a
@@ -244,6 +252,7 @@ __device__ __forceinline__ void flux_tile(const Inst& I, const Tile& t, int stag
 #pragma unroll 1
     for (int h = 0; h < FLUX_FACES / 32; ++h) {
         const int f = lane + 32 * h;
+        const int c = (int)(((h ? kC1 : kC0) >> (4 * w)) & 15u); // warp-uniform
         if (S.act[f]) {
             int i, j, p0, ps;
             face_index<DIR>(t, f, i, j, p0, ps);
@@ -251,11 +260,12 @@ __device__ __forceinline__ void flux_tile(const Inst& I, const Tile& t, int stag
         }
     }
     __syncthreads();
-    // ---- 3. output pass: component k = c
+    // ---- 3. output pass: component k of faces lane and lane + 32
 #pragma unroll 1
     for (int h = 0; h < FLUX_FACES / 32; ++h) {
         const int f = lane + 32 * h;
-        if (S.act[f]) face_out<DIR>(I, S, t, c, f);
+        const int k = h ? (w + 3) % 6 : w;
+        if (S.act[f]) face_out<DIR>(I, S, t, k, f);
     }
 }
 

@@ -351,8 +351,18 @@ __device__ __forceinline__ RoeDiv roe_div(const Roe& q, const DevParams& P) {
     RoeDiv r;
     r.den = recip(q.den);
     r.b = recip(q.b);
-    r.c6 = recip(6.0 * q.cs2);
-    r.c3 = recip(3.0 * q.cs2);
+    // den = RN(12 cs2) is exactly 2 RN(6 cs2) and 4 RN(3 cs2) (scaling by a
+    // power of two commutes with rounding), so while den is in the fast range
+    // (no overflow or underflow) RN(1 / (6 cs2)) = 2 RN(1 / den) and
+    // RN(1 / (3 cs2)) = 4 RN(1 / den) exactly: two IEEE divisions fewer
+    if (r.den.ok) {
+        const double c6 = 6.0 * q.cs2, c3 = 3.0 * q.cs2;
+        r.c6 = {c6, 2.0 * r.den.y, div_in_range(c6)};
+        r.c3 = {c3, 4.0 * r.den.y, div_in_range(c3)};
+    } else {
+        r.c6 = recip(6.0 * q.cs2);
+        r.c3 = recip(3.0 * q.cs2);
+    }
     r.cg = recip(gt * q.cs2);
     r.gt = recip(gt);
     return r;

@@ -381,10 +381,12 @@ int rh3t_math_check(int32_t device, const double* x, int32_t n, double q, double
  * the solver uses in place of IEEE division where one divisor serves several
  * quotients (Markstein's correction step from y = RN(1/b); the constants 3
  * and 6) against the IEEE quotient, bit for bit, on n device-generated
- * operand pairs: counts[0..5] the mismatches per category (0 random,
+ * operand pairs: counts[0..6] the mismatches per category (0 random,
  * 1 divisors with all-ones significands, 2 quotients next to a rounding
- * midpoint, 3 range edges and special values, 4 a / 3, 5 a / 6);
- * first[3] = a, b and the routine's quotient of one mismatch. */
+ * midpoint, 3 range edges and special values, 4 a / 3, 5 a / 6, 6 the
+ * reciprocals of a face's 6 c^2 and 3 c^2, formed as 2 and 4 times
+ * RN(1 / (12 c^2))); first[3] = a, b and the routine's quotient of one
+ * mismatch. */
 int rh3t_div_check(int32_t device, int64_t n, uint64_t seed, int64_t* counts, double* first);
 
 /* Diagnostic (no reference counterpart): the bounded mbarrier wait of the

@@ -35,10 +35,11 @@ def test_shared_reciprocal_division_bitwise(rh):
     bit. 4e9 device-generated pairs: random operands over the fast path's
     exponent range and beyond it, divisors with all-ones significands,
     quotients next to a rounding midpoint, special values, and the two
-    constants."""
+    constants; and the face's reciprocals of 6 c^2 and 3 c^2, which the
+    flux kernel forms as 2 and 4 times RN(1 / (12 c^2))."""
     for exact in (True, False):
         L = rh.load(exact)
-        counts = np.zeros(6, np.int64)
+        counts = np.zeros(7, np.int64)
         first = np.zeros(3)
         seed = 1 if exact else 2
         assert L.rh3t_div_check(0, 2_000_000_000, seed, counts.ctypes.data, first.ctypes.data) == 0
