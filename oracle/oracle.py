@@ -124,12 +124,23 @@ def lib():
             ("oracle_reconstruction_slow", None, [dp, I, I, dp, dp]),
             ("oracle_ghost_probe", I, [P, LG, LG, dp]),
             ("oracle_ghost_value_at", I, [P, LG, LG, dp, I, I, I, dp]),
+            ("oracle_wall_systems", I, [P, LG, dp, dp, dp, dp]),
+            ("oracle_solve6", I, [dp, dp, dp]),
         ]:
             f = getattr(L, name)
             f.restype = res
             f.argtypes = args
         _lib = L
     return _lib
+
+
+def solve6(A, b):
+    """bc1.rs:467-469 solve6 as the oracle restates it (LU with partial
+    pivoting); None for a zero pivot."""
+    A = np.ascontiguousarray(A, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    x = np.zeros(6)
+    return None if lib().oracle_solve6(_dp(A), _dp(b), _dp(x)) else x
 
 
 def _ptr(a):
@@ -336,6 +347,16 @@ class Case:
         if lib().oracle_ghost_extrapolation(self.h, gid, _dp(out)):
             raise ValueError("not a WENO-extrapolated ghost")
         return out
+
+    def wall_systems(self, gid):
+        """The two 6x6 ILW systems (A0, b0, A1, b1) of Wall ghost gid as the
+        ghost update solves them (bc1.rs:691-740); None when the first is
+        singular."""
+        A0, A1, b0, b1 = np.zeros((6, 6)), np.zeros((6, 6)), np.zeros(6), np.zeros(6)
+        rc = lib().oracle_wall_systems(self.h, gid, _dp(A0), _dp(b0), _dp(A1), _dp(b1))
+        if rc < 0:
+            raise ValueError("not a Wall ghost")
+        return None if rc else (A0, b0, A1, b1)
 
     def extractor(self, proj5, r):
         out = np.zeros(((r + 1) ** 2, 2), np.int32)

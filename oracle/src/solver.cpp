@@ -215,24 +215,37 @@ static State set_ghost_point_value(const GhostInfo& g, const Field& f, const Sta
 // characteristic derivatives v[k] (k = 0..4) and L, R, lambda at the nearest
 // node, then the Taylor sum to the ghost point (shared by the precomputed
 // path above and the per-call path of slowpath.cpp, as in the reference).
+// bc1.rs:691-702 the first ILW system of a Wall ghost: L with its first row
+// replaced by the no-penetration row, right-hand side v^(0) with a zero first
+// entry
+static void wall_system0(const double L[6][6], const double v[5][6], double A0[6][6], double rhs0[6]) {
+    std::memcpy(A0, L, 36 * sizeof(double));
+    for (int c = 0; c < 6; ++c) A0[0][c] = c == 1 ? 1.0 : 0.0;
+    for (int c = 0; c < 6; ++c) rhs0[c] = v[0][c];
+    rhs0[0] = 0.0;
+}
+// bc1.rs:703-740 the second: L with the ILW momentum row at u^(0) first
+static void wall_system1(const double L[6][6], const double v[5][6], const double u0[6], const Params& P,
+                         double A1[6][6], double rhs1[6]) {
+    double row1[6];
+    std::memcpy(A1, L, 36 * sizeof(double));
+    build_ilw_row1(u0, P, row1);
+    for (int c = 0; c < 6; ++c) A1[0][c] = row1[c];
+    for (int c = 0; c < 6; ++c) rhs1[c] = v[1][c];
+    rhs1[0] = 0.0;
+}
+
 State ghost_from_extrapolation(const BC& bc, const Projection& pr, const double L[6][6], const double R[6][6],
                                const double lam[6], const double v[5][6], const Params& P, long gi, long gj) {
     double u[5][6];
     if (bc.kind == BC_WALL) {
         // bc1.rs:691-756
         double A0[6][6], rhs0[6];
-        std::memcpy(A0, L, sizeof(A0));
-        for (int c = 0; c < 6; ++c) A0[0][c] = c == 1 ? 1.0 : 0.0;
-        for (int c = 0; c < 6; ++c) rhs0[c] = v[0][c];
-        rhs0[0] = 0.0;
+        wall_system0(L, v, A0, rhs0);
         if (!solve6(A0, rhs0)) throw OracleError(ERR_SINGULAR, "singular ILW/extrapolation system at boundary", gi, gj);
         for (int c = 0; c < 6; ++c) u[0][c] = rhs0[c];
-        double A1[6][6], rhs1[6], row1[6];
-        std::memcpy(A1, L, sizeof(A1));
-        build_ilw_row1(u[0], P, row1);
-        for (int c = 0; c < 6; ++c) A1[0][c] = row1[c];
-        for (int c = 0; c < 6; ++c) rhs1[c] = v[1][c];
-        rhs1[0] = 0.0;
+        double A1[6][6], rhs1[6];
+        wall_system1(L, v, u[0], P, A1, rhs1);
         if (!solve6(A1, rhs1)) throw OracleError(ERR_SINGULAR, "singular ILW/extrapolation system at boundary", gi, gj);
         for (int c = 0; c < 6; ++c) u[1][c] = rhs1[c];
         for (int k = 2; k <= 4; ++k) mat_vec(R, v[k], u[k]);
@@ -1340,6 +1353,40 @@ int oracle_ghost_extrapolation(void* h, long id, double* v30) {
     build_local_plain(g.project.normal, s.f.value[s.f.linear_index(pre.nearest_i, pre.nearest_j)], s.P, L, R, lam);
     weno_extrapolation_all(L, pre, s.f.value.data(), s.P, v);
     std::memcpy(v30, v, sizeof(v));
+    return 0;
+}
+// The two ILW systems of Wall ghost `id` as the ghost update hands them to
+// solve6 (bc1.rs:691-740; the second is formed at the first one's solution),
+// row-major; returns -1 for a ghost that is not a Wall ghost, 1 when the
+// first system is singular, 0 otherwise.
+int oracle_wall_systems(void* h, long id, double* A0, double* b0, double* A1, double* b1) {
+    Solver& s = ((Handle*)h)->s;
+    const GhostInfo& g = s.gg.info[id];
+    if (g.pre < 0) return -1;
+    const BC& bc = (g.boundary == OUTER ? s.f.bc_outer : s.f.bc_inner)[g.side_id];
+    if (bc.kind != BC_WALL) return -1;
+    const GhostBC& pre = s.gg.pre[g.pre];
+    double L[6][6], R[6][6], lam[6], v[5][6];
+    build_local_plain(g.project.normal, s.f.value[s.f.linear_index(pre.nearest_i, pre.nearest_j)], s.P, L, R, lam);
+    weno_extrapolation_all(L, pre, s.f.value.data(), s.P, v);
+    double M0[6][6], r0[6], M1[6][6], r1[6];
+    wall_system0(L, v, M0, r0);
+    std::memcpy(A0, M0, sizeof(M0));
+    std::memcpy(b0, r0, sizeof(r0));
+    if (!solve6(M0, r0)) return 1;
+    wall_system1(L, v, r0, s.P, M1, r1);
+    std::memcpy(A1, M1, sizeof(M1));
+    std::memcpy(b1, r1, sizeof(r1));
+    return 0;
+}
+// bc1.rs:467-469 solve6 on one system (row-major A, right-hand side b):
+// x = A^-1 b; returns 0, or 1 when the LU factorisation meets a zero pivot
+int oracle_solve6(const double* A36, const double* b6, double* x6) {
+    double A[6][6], b[6];
+    std::memcpy(A, A36, sizeof(A));
+    std::memcpy(b, b6, sizeof(b));
+    if (!solve6(A, b)) return 1;
+    std::memcpy(x6, b, sizeof(b));
     return 0;
 }
 // weno.rs:599-679 Stencil6::reconstruction (the ndarray variant)
