@@ -32,11 +32,6 @@ constexpr bool kExact = true;
 constexpr bool kExact = false;
 #endif
 
-__device__ __forceinline__ double weno5_any(double a, double b, double c, double d, double e, double eps) {
-    if (kExact) return weno5(a, b, c, d, e, eps);
-    return fastm::weno5(a, b, c, d, e, eps);
-}
-
 // Roe state: u v w2 ee ei er cs2 cs he hi hr b den, then the reciprocals
 // the L rows divide by: FMA build 1/cs2, 1/b; no-contraction build RN(1/d)
 // of d = den, b, 6 cs2, 3 cs2, gt cs2 (their quotients stay the IEEE ones)
@@ -106,7 +101,8 @@ __device__ __forceinline__ double char_flux(const FluxShared& S, const DevParams
         fm[k] = 0.5 * (cf - a * cs);
     }
     if (!kExact)
-        return weno5_any(fp[0], fp[1], fp[2], fp[3], fp[4], P.eps) + weno5_any(fm[5], fm[4], fm[3], fm[2], fm[1], P.eps);
+        return fastm::weno5(fp[0], fp[1], fp[2], fp[3], fp[4], P.eps) +
+               fastm::weno5(fm[5], fm[4], fm[3], fm[2], fm[1], P.eps);
     // no-contraction build: the two reconstructions as a two-pass loop over
     // one inlined WENO5 (one copy of its code, no call: the out-of-line
     // version spilled registers around each of its calls and ran 3% slower)
